@@ -1,0 +1,455 @@
+#!/usr/bin/env python
+"""HMC trajectories/hour at L=48, Ltau=480 (mixed precision) on B200.
+
+One step = one HMC trajectory (Metropolis update) of every chain: 20 leapfrog
+steps of size 0.05, dtau = 0.1, J = K = 1, PCG on M^dag M to relative residual
+1e-10 (float iterations, double reliable updates every <= 50 iterations), the
+reference's physical start (staggered pi-flux +-pi/4 plus Gaussian noise).
+The line also reports, measured in the same run: the plain FP64 path's
+trajectories/hour, Delta H of one shared trajectory in both precisions, the
+M^dag M matvec bandwidth, and the roofline of the dominant kernel (the
+persistent PCG).  ``--impl reference`` times the CPU restatement of the
+reference's path (the oracle) on the host cores instead.
+
+Multi-GPU (torchrun): replicas only -- every rank runs its own chains, no
+data-path collective; the timed region is bracketed by barriers and the
+maximum over ranks is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "HMC trajectories/hour at L=48, Ltau=480 (mixed precision, Delta H checked against FP64)"
+UNIT = "trajectories/hour"
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--L", type=int, default=48)
+    ap.add_argument("--Ltau", type=int, default=480)
+    ap.add_argument("--bs", type=int, default=2, help="chains per GPU")
+    ap.add_argument("--n-leapfrog", type=int, default=20)
+    ap.add_argument("--delta-t", type=float, default=0.05)
+    ap.add_argument("--rtol", type=float, default=1e-10)
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--mhm-rhs", type=int, default=8)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cg-iters-per-solve", type=float, default=None,
+                    help="reference arm: PCG iterations per solve used to extrapolate a trajectory")
+    ap.add_argument("--seed", type=int, default=1234)
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id):
+        self.bus_id = bus_id
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+            if self.bus_id:
+                cmd += ["-i", self.bus_id]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline: the oracle (CPU restatement of the reference)
+# ---------------------------------------------------------------------------
+def cpu_sample(L, Ltau, seed, seconds):
+    """Time the CPU restatement on the same lattice: PCG iterations (M^dag M,
+    preconditioner, axpys, dots) and one fermion force.  Returns per-unit
+    seconds and what was sampled."""
+    import numpy as np
+    from oracle import qedf_oracle as O
+    rng = np.random.default_rng(seed)
+    Vs = L * L
+    boson = pi_flux_np(rng, L, Ltau, 1)
+    phi = O.ref_to_kernel_layout(boson)
+    v = (rng.standard_normal((1, Ltau, Vs)) + 1j * rng.standard_normal((1, Ltau, Vs))) / math.sqrt(2)
+    P = O.precon_tau_matrix(Ltau) if Ltau >= O.precon_min_ltau() else None
+    t0 = time.perf_counter()
+    n_it = 0
+    x = np.zeros_like(v)
+    r = v.copy()
+    p = r.copy()
+    while True:
+        Op = O.mhm_vec(phi, p, L, 0.1)
+        a = np.vdot(r, r).real / np.vdot(p, Op).real
+        x = x + a * p
+        r = r - a * Op
+        z = O.precon_vec(r, P) if P is not None else r
+        b = np.vdot(r, z).real
+        p = z + 0.5 * p
+        n_it += 1
+        if time.perf_counter() - t0 > seconds * 0.6 and n_it >= 1:
+            break
+    t_it = (time.perf_counter() - t0) / n_it
+    t1 = time.perf_counter()
+    n_f = 0
+    while True:
+        O.force_f_from_xi(phi, v, L, 0.1)
+        n_f += 1
+        if time.perf_counter() - t1 > seconds * 0.3:
+            break
+    t_force = (time.perf_counter() - t1) / n_f
+    return t_it, t_force, f"{n_it} PCG iterations + {n_f} fermion forces of the numpy oracle at L={L}, Ltau={Ltau}"
+
+
+def cpu_traj_per_hour(t_it, t_force, iters_per_solve, n_leapfrog):
+    solves = n_leapfrog + 1
+    t_traj = solves * (iters_per_solve * t_it + t_force)
+    return 3600.0 / t_traj
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    iters = args.cg_iters_per_solve
+    if iters is None:
+        iters = float(os.environ.get("QEDF_CG_ITERS_PER_SOLVE", "250"))
+    per_step = []
+    sample = ""
+    for k in range(args.warmup + args.steps):
+        t_it, t_force, sample = cpu_sample(args.L, args.Ltau, args.seed + k, args.cpu_seconds / 2)
+        if k >= args.warmup:
+            per_step.append(cpu_traj_per_hour(t_it, t_force, iters, args.n_leapfrog))
+    value = statistics.median(per_step)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3600e3 / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64 (numpy)",
+        "data": "synthetic", "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": sample + f"; extrapolated with {iters:g} PCG iterations per solve, "
+                                            f"{args.n_leapfrog + 1} solves + forces per trajectory"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args):
+    return {"workload": f"HMC trajectory L={args.L} Ltau={args.Ltau} dtau=0.1 J=1 K=1, {args.n_leapfrog} leapfrog "
+                        f"steps of {args.delta_t}, PCG rtol {args.rtol}, {args.bs} chains per GPU",
+            "lattice": [args.L, args.L, args.Ltau], "chains_per_gpu": args.bs, "n_leapfrog": args.n_leapfrog,
+            "delta_t": args.delta_t, "cg_rtol": args.rtol, "precision": "mixed (float CG, double reliable "
+            "updates / H / Metropolis)", "l2": "inputs larger than L2 (per-GPU working set > 126 MB)",
+            "init": "staggered pi-flux +-pi/4 plus Gaussian noise (reference's physical start)"}
+
+
+def pi_flux_np(rng, L, Ltau, bs):
+    import numpy as np
+    x = np.arange(L)[:, None]
+    y = np.arange(L)[None, :]
+    sg = 1 - 2 * ((x + y) % 2)
+    b = np.zeros((bs, 2, L, L, Ltau))
+    b[:, 0] = (sg * math.pi / 4)[None, :, :, None]
+    b[:, 1] = (-sg * math.pi / 4)[None, :, :, None]
+    return b + 0.05 * rng.standard_normal(b.shape)
+
+
+# ---------------------------------------------------------------------------
+# native arm
+# ---------------------------------------------------------------------------
+def run_native(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    from qed_fermion_b200 import _lib, build, ops
+    from qed_fermion_b200.hmc import HmcSampler, ref_to_kernel
+    build.build()
+    L, Lt, bs = args.L, args.Ltau, args.bs
+    seed = args.seed + 1000 * rank
+    rng = np.random.default_rng(seed)
+
+    def make(precision):
+        h = HmcSampler(Lx=L, Ltau=Lt, J=1.0, K=1.0, dtau=0.1, bs=bs, delta_t=args.delta_t,
+                       N_leapfrog=args.n_leapfrog, precision=precision, cg_rtol=args.rtol, max_iter=20000,
+                       device=dev, seed=seed)
+        return h
+
+    hmc = make("mixed")
+    boson0 = torch.tensor(pi_flux_np(rng, L, Lt, bs), device=dev)
+    hmc.boson = boson0.to(torch.float32)
+    stream = torch.cuda.current_stream()
+
+    # --- instrumentation of the persistent PCG launches (events on the stream)
+    solve_events = []
+    orig_solve = hmc.solver.solve
+
+    def timed_solve(*a, **k):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = orig_solve(*a, **k)
+        e1.record(stream)
+        solve_events.append((e0, e1, res.iters))
+        return res
+
+    hmc.solver.solve = timed_solve
+
+    # --- warm-up
+    for _ in range(args.warmup):
+        hmc.metropolis_update()
+    torch.cuda.synchronize()
+    solve_events.clear()
+
+    # --- timed region (device residency: inputs already in HBM)
+    bus = None
+    try:
+        pci = torch.cuda.get_device_properties(dev)
+        bus = f"{pci.pci_domain_id:08X}:{pci.pci_bus_id:02X}:{pci.pci_device_id:02X}.0"
+    except Exception:
+        bus = None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = _lib.LAUNCHES["count"]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    accepted = []
+    with ClockSampler(bus) as clk:
+        t_start.record(stream)
+        for _ in range(args.steps):
+            _, accp, it, err, H0, H1 = hmc.metropolis_update()
+            accepted.append(accp)
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    launches = _lib.LAUNCHES["count"] - launches0
+    elapsed = t_start.elapsed_time(t_end) / 1e3
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t)
+        dist.barrier()
+    value = 3600.0 * args.steps * bs * world / elapsed
+    clocks = clk.summary()
+    acc_rate = float(torch.stack(accepted).double().mean())
+
+    # --- dominant kernel: the persistent PCG (algorithmic bytes per launch)
+    N = L * L * Lt
+    pcg_ms, pcg_bytes, iters_all = [], [], []
+    for e0, e1, its in solve_events:
+        ms = e0.elapsed_time(e1)
+        it_sum = int(its.sum())
+        iters_all.extend(its.cpu().tolist())
+        pcg_ms.append(ms)
+        pcg_bytes.append(it_sum * N * (7 * 8 + 2 * 4))  # float vectors and angles per iteration
+    pcg_time = sum(pcg_ms) / 1e3
+    achieved = sum(pcg_bytes) / pcg_time / 1e9 if pcg_time > 0 else None
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_kind = "measured" if "hbm_gbs" in peaks else "fallback"
+
+    result = {}
+    if rank == 0:
+        result["pcg_share_of_step"] = pcg_time / elapsed
+        result["cg_iters_per_solve"] = statistics.mean(iters_all) if iters_all else None
+
+    # --- end to end through the public API with host buffers
+    e2e = None
+    if rank == 0:
+        hb = torch.empty((bs, 2, L, L, Lt), dtype=torch.float32, pin_memory=True)
+        hb.copy_(hmc.boson.cpu())
+        hout = torch.empty_like(hb).pin_memory()
+        hH = torch.empty((3, bs), dtype=torch.float64, pin_memory=True)
+        k_e2e = max(1, min(args.steps, 2))
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k_e2e):
+            hmc.boson = hb.to(dev, non_blocking=True)
+            _, accp, it, err, H0, H1 = hmc.metropolis_update()
+            hout.copy_(hmc.boson, non_blocking=True)
+            hH[0].copy_(H0, non_blocking=True)
+            hH[1].copy_(H1, non_blocking=True)
+            hH[2].copy_(accp.double(), non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_e2e = e0.elapsed_time(e1) / 1e3
+        e2e = {"value": 3600.0 * k_e2e * bs / t_e2e, "unit": UNIT, "h2d_bytes_per_step": hb.numel() * 4,
+               "d2h_bytes_per_step": hout.numel() * 4 + hH.numel() * 8, "steps": k_e2e}
+
+    # --- plain FP64 path, same workload
+    fp64 = None
+    if rank == 0 and args.fp64_steps > 0:
+        h64 = make("fp64")
+        h64.boson = hmc.boson.to(torch.float64)
+        h64.metropolis_update()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.fp64_steps):
+            h64.metropolis_update()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t64 = e0.elapsed_time(e1) / 1e3
+        fp64 = {"value": 3600.0 * args.fp64_steps * bs / t64, "unit": UNIT, "steps": args.fp64_steps,
+                "s_per_trajectory": t64 / args.fp64_steps}
+
+    # --- Delta H of one shared trajectory, mixed vs FP64
+    dH = None
+    if rank == 0:
+        h64 = make("fp64")
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(seed + 7)
+        x0 = hmc.boson.to(torch.float64)
+        p0 = torch.randn(x0.shape, device=dev, dtype=torch.float64, generator=gen)
+        R = torch.randn((bs, N), device=dev, dtype=torch.complex128, generator=gen) / math.sqrt(2)
+        _, H0m, H1m, _, _ = hmc.leapfrog_proposer5(x0.to(torch.float32), p0=p0.to(torch.float32), R=R)
+        _, H0d, H1d, _, _ = h64.leapfrog_proposer5(x0.to(torch.float32).to(torch.float64),
+                                                    p0=p0.to(torch.float32).to(torch.float64), R=R)
+        dHm, dHd = (H1m - H0m).cpu(), (H1d - H0d).cpu()
+        dH = {"dH_mixed": dHm.tolist(), "dH_fp64": dHd.tolist(),
+              "abs_err": (dHm - dHd).abs().tolist(),
+              "rel_err_vs_H0": ((dHm - dHd).abs() / H0d.abs().cpu()).tolist(), "H0": H0d.cpu().tolist()}
+
+    # --- M^dag M matvec bandwidth (several right-hand sides, working set > L2)
+    mhm = None
+    if rank == 0:
+        nr = args.mhm_rhs
+        mhm = {}
+        for prec, cdt, rdt, bps in (("c64", torch.complex64, torch.float32, 24), ("c128", torch.complex128,
+                                                                                 torch.float64, 48)):
+            phi = torch.rand((nr, 2 * N), device=dev, dtype=rdt) * 6.28 - 3.14
+            xv = torch.randn((nr, N), device=dev, dtype=cdt)
+            out = torch.empty_like(xv)
+            for _ in range(3):
+                ops.apply_operator("mhm", phi, xv, L, 0.1, out=out)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            reps = 10
+            e0.record(stream)
+            for _ in range(reps):
+                ops.apply_operator("mhm", phi, xv, L, 0.1, out=out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            gbs = bps * N * nr / (ms / 1e3) / 1e9
+            mhm[prec] = {"GBps": gbs, "frac_of_measured_hbm": gbs / hbm_peak, "ms_per_launch": ms,
+                         "rhs": nr, "bytes_per_site": bps}
+            del phi, xv, out
+
+    # --- CPU baseline (oracle restatement) on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1:
+        t_it, t_force, sample = cpu_sample(L, Lt, seed, args.cpu_seconds)
+        ips = result.get("cg_iters_per_solve") or 250
+        cpu = {"value": cpu_traj_per_hour(t_it, t_force, ips, args.n_leapfrog), "unit": UNIT, "cores": 1,
+               "kind": "port", "sample": sample + f"; extrapolated with the {ips:.0f} PCG iterations per solve "
+                                                  f"this run needed, {args.n_leapfrog + 1} solves per trajectory",
+               "s_per_cg_iteration": t_it, "s_per_force": t_force}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (c64) iterations, f64 reliable updates/H",
+            "data": "synthetic", "config": workload_config(args),
+            "roofline": {"bound": "hbm", "kernel": "k_pcg (persistent batched PCG)",
+                         "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": (achieved / hbm_peak) if achieved else None, "peak_kind": peak_kind,
+                         "traffic": None,
+                         "bytes_model": "per PCG iteration per rhs: N*(7*8 + 2*4) B (read p,x,r,angles; write x,r,p)"},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+            "fp64_plain": fp64, "speedup_vs_fp64": (value / bs / world * bs) / fp64["value"] if fp64 else None,
+            "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate, **result,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_native(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

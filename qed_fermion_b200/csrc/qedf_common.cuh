@@ -1,0 +1,152 @@
+// Common device helpers for the qed_fermion B200 kernels.
+//
+// Complex numbers are stored interleaved (re, im), the layout of torch
+// complex64 / complex128, so vectors are passed as plain float / double
+// pointers of twice the length.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/qedf.h"
+
+namespace qedf {
+
+template <typename R>
+struct Cx {
+  R re, im;
+};
+
+template <typename R>
+__host__ __device__ __forceinline__ Cx<R> mk(R a, R b) {
+  Cx<R> z;
+  z.re = a;
+  z.im = b;
+  return z;
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> operator+(Cx<R> a, Cx<R> b) { return mk<R>(a.re + b.re, a.im + b.im); }
+template <typename R>
+__device__ __forceinline__ Cx<R> operator-(Cx<R> a, Cx<R> b) { return mk<R>(a.re - b.re, a.im - b.im); }
+template <typename R>
+__device__ __forceinline__ Cx<R> operator*(R s, Cx<R> a) { return mk<R>(s * a.re, s * a.im); }
+template <typename R>
+__device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
+  return mk<R>(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+// conj(a) * b
+template <typename R>
+__device__ __forceinline__ Cx<R> cjmul(Cx<R> a, Cx<R> b) {
+  return mk<R>(a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re);
+}
+// a + m * b
+template <typename R>
+__device__ __forceinline__ Cx<R> cfma(Cx<R> m, Cx<R> b, Cx<R> a) {
+  Cx<R> z;
+  z.re = fma(m.re, b.re, fma(-m.im, b.im, a.re));
+  z.im = fma(m.re, b.im, fma(m.im, b.re, a.im));
+  return z;
+}
+// a + conj(m) * b
+template <typename R>
+__device__ __forceinline__ Cx<R> cjfma(Cx<R> m, Cx<R> b, Cx<R> a) {
+  Cx<R> z;
+  z.re = fma(m.re, b.re, fma(m.im, b.im, a.re));
+  z.im = fma(m.re, b.im, fma(-m.im, b.re, a.im));
+  return z;
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> cneg(Cx<R> a) { return mk<R>(-a.re, -a.im); }
+
+// e^{i x} scaled by t.  Single precision: the argument is first reduced to
+// [-pi, pi] (two-constant Cody-Waite reduction with 2*pi split into its
+// float value and the remainder), then the hardware approximations
+// __sinf/__cosf are used, whose maximum absolute error on [-pi, pi] is
+// documented as 2^-21.41 (sin) and 2^-21.19 (cos).  The phase always enters
+// multiplied by tanh(dtau/2) <= tanh(dtau), so its contribution to an
+// operator application is below 1e-7 relative for dtau <= 0.1.
+__device__ __forceinline__ Cx<float> tphase(float x, float t) {
+  const float k = rintf(x * 0.15915494309189535f);
+  float r = fmaf(-k, 6.28318548202514648f, x);
+  r = fmaf(-k, -1.7484556000744487e-07f, r);
+  float s, c;
+  __sincosf(r, &s, &c);
+  return mk<float>(t * c, t * s);
+}
+// Double precision: CUDA's sincos().
+__device__ __forceinline__ Cx<double> tphase(double x, double t) {
+  double s, c;
+  sincos(x, &s, &c);
+  return mk<double>(t * c, t * s);
+}
+
+// Vector loads/stores of two consecutive complex numbers (16 B for complex64,
+// 32 B for complex128).  Addresses are 16-byte aligned by construction: the
+// first site of each pair has an even x and L is even.
+__device__ __forceinline__ void ld2(const float* p, Cx<float>& a, Cx<float>& b) {
+  float4 q = __ldg(reinterpret_cast<const float4*>(p));
+  a = mk<float>(q.x, q.y);
+  b = mk<float>(q.z, q.w);
+}
+__device__ __forceinline__ void ld2(const double* p, Cx<double>& a, Cx<double>& b) {
+  double2 q0 = __ldg(reinterpret_cast<const double2*>(p));
+  double2 q1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  a = mk<double>(q0.x, q0.y);
+  b = mk<double>(q1.x, q1.y);
+}
+// plain (coherent) loads for buffers written earlier in the same kernel
+__device__ __forceinline__ void ld2c(const float* p, Cx<float>& a, Cx<float>& b) {
+  float4 q = *reinterpret_cast<const float4*>(p);
+  a = mk<float>(q.x, q.y);
+  b = mk<float>(q.z, q.w);
+}
+__device__ __forceinline__ void ld2c(const double* p, Cx<double>& a, Cx<double>& b) {
+  double2 q0 = *reinterpret_cast<const double2*>(p);
+  double2 q1 = *(reinterpret_cast<const double2*>(p) + 1);
+  a = mk<double>(q0.x, q0.y);
+  b = mk<double>(q1.x, q1.y);
+}
+__device__ __forceinline__ void st2(float* p, Cx<float> a, Cx<float> b) {
+  *reinterpret_cast<float4*>(p) = make_float4(a.re, a.im, b.re, b.im);
+}
+__device__ __forceinline__ void st2(double* p, Cx<double> a, Cx<double> b) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(a.re, a.im);
+  reinterpret_cast<double2*>(p)[1] = make_double2(b.re, b.im);
+}
+// four reals (angles or forces of two sites, both components)
+__device__ __forceinline__ void ld4(const float* p, float (&a)[4]) {
+  float4 q = __ldg(reinterpret_cast<const float4*>(p));
+  a[0] = q.x; a[1] = q.y; a[2] = q.z; a[3] = q.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double (&a)[4]) {
+  double2 q0 = __ldg(reinterpret_cast<const double2*>(p));
+  double2 q1 = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  a[0] = q0.x; a[1] = q0.y; a[2] = q1.x; a[3] = q1.y;
+}
+__device__ __forceinline__ void st4(float* p, const float (&a)[4]) {
+  *reinterpret_cast<float4*>(p) = make_float4(a[0], a[1], a[2], a[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double (&a)[4]) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(a[0], a[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(a[2], a[3]);
+}
+
+// Coefficients of the checkerboard factors F_g = c_g (I + t_g K_g):
+// g1 uses cosh/tanh(dtau), g2..g4 cosh/tanh(dtau/2); Cb = c1 c2^2 c3^2 c4^2
+// is the scalar that B = F4 F3 F2 F1 F2 F3 F4 carries in front of the
+// product of the unscaled factors.
+struct FactorCoeffs {
+  double c1, ch, t1, th, Cb;
+};
+
+inline FactorCoeffs factor_coeffs(double dtau) {
+  FactorCoeffs f;
+  f.c1 = cosh(dtau);
+  f.ch = cosh(dtau / 2);
+  f.t1 = tanh(dtau);
+  f.th = tanh(dtau / 2);
+  f.Cb = f.c1 * f.ch * f.ch * f.ch * f.ch * f.ch * f.ch;
+  return f;
+}
+
+}  // namespace qedf

@@ -1,0 +1,797 @@
+// Persistent batched preconditioned CG on M^dag M x = b.
+//
+// One cooperative launch runs the whole solve.  Each iteration is two
+// grid-wide phases separated by grid barriers:
+//
+//   A  (operator units: one right-hand side x one tau-slab)
+//        p_new = z + beta p_old          (halo slices recomputed, not exchanged)
+//        Op    = M^dag M p_new            (slice engine, registers + smem)
+//        pAp  += Re p_new^dag Op          (double)
+//   BC (elementwise units: one right-hand side x a chunk of sites, all tau)
+//        x += alpha p_new,  r -= alpha Op
+//        z  = (P_tau (x) I) r             (the chunk's r column stays in smem)
+//        rr += |r|^2,  rz += Re r^dag z   (double)
+//
+// which is the arithmetic of preconditioned_cg_fast_test
+// (hmc_sampler_batch.py:751-846) with the reference's per-iteration torch
+// kernels (einsum dots, axpys, _C.mhm_vec, _C.precon_vec) fused.  Every
+// right-hand side has its own mask: once ||r||/||b|| <= rtol it stops
+// updating (the reference's active_bs, :826).
+//
+// Mixed mode iterates in float and keeps x and b in double: x_lo (float)
+// accumulates the update, and a reliable update folds it into x (double),
+// recomputes the true residual r = b - A x with the double-precision engine
+// and restarts r from it.  It runs every ru_interval iterations, when the
+// iterated residual fell by ru_delta since the last one, and whenever the
+// iterated residual claims convergence, so convergence is always decided on
+// the true residual.
+//
+// Per-right-hand-side scalars (alpha, beta, masks) are recomputed by every
+// thread block from the same double accumulators in the same order, so all
+// blocks take identical decisions without another barrier.  Grid barriers
+// spin with a clock budget; when it runs out the block raises an error flag
+// that ends every block's loop, and the solve reports QEDF_ERR_TIMEOUT.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+
+#include "qedf_internal.h"
+#include "qedf_precon_table.h"
+#include "qedf_slice.cuh"
+
+namespace qedf {
+
+__constant__ PreTable c_pre = {QEDF_PRE_LAYOUT, QEDF_PRE_EDGE_VALUES, QEDF_PRE_TAIL_VALUES,
+                               QEDF_PRE_MIDDLE_VALUES, QEDF_PRE_CORNER_VALUES};
+static const PreTable h_pre = {QEDF_PRE_LAYOUT, QEDF_PRE_EDGE_VALUES, QEDF_PRE_TAIL_VALUES,
+                               QEDF_PRE_MIDDLE_VALUES, QEDF_PRE_CORNER_VALUES};
+
+// ---------------------------------------------------------------------------
+// bounded grid barrier
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, long long budget) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* gen = bar + 1;
+    volatile unsigned int* err = bar + 2;
+    const unsigned int g = *gen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(bar, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (*gen == g) {
+        if (*err) break;
+        if (clock64() - t0 > budget) {
+          atomicExch(bar + 2, (unsigned int)QEDF_ERR_TIMEOUT);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *((volatile unsigned int*)(bar + 2)) == 0;
+}
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// sum over the block, result valid in thread 0
+__device__ double block_sum_d(double v, double* sh) {
+  v = warp_sum_d(v);
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  __syncthreads();
+  if (ln == 0) sh[w] = v;
+  __syncthreads();
+  double t = 0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x + 31) / 32 ? sh[threadIdx.x] : 0.0;
+    t = warp_sum_d(t);
+  }
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// accumulator layout (doubles)
+// ---------------------------------------------------------------------------
+struct Acc {
+  double* bb;       // [NV]
+  double* pAp;      // [2][NV]
+  double* rr;       // [2][NV]
+  double* rz;       // [2][NV]
+  double* ru_rr;    // [NV]
+  double* ru_rz;    // [NV]
+  __device__ Acc(double* a, int NV) {
+    bb = a;
+    pAp = a + NV;
+    rr = a + 3 * NV;
+    rz = a + 5 * NV;
+    ru_rr = a + 7 * NV;
+    ru_rz = a + 8 * NV;
+  }
+};
+constexpr int ACC_PER_RHS = 9;
+
+// unit -> system
+__device__ __forceinline__ int find_sys_A(const PcgParams& p, int u) {
+  int s = 0;
+  while (s + 1 < p.nsys && u >= p.sys[s + 1].unitA0) ++s;
+  return s;
+}
+__device__ __forceinline__ int find_sys_E(const PcgParams& p, int u) {
+  int s = 0;
+  while (s + 1 < p.nsys && u >= p.sys[s + 1].unitE0) ++s;
+  return s;
+}
+
+template <typename R>
+__device__ __forceinline__ Cx<R> ldc(const R* base, int64_t i) {
+  return mk<R>(base[2 * i], base[2 * i + 1]);
+}
+template <typename R>
+__device__ __forceinline__ void stc(R* base, int64_t i, Cx<R> v) {
+  base[2 * i] = v.re;
+  base[2 * i + 1] = v.im;
+}
+
+// Per-block copy of the per-right-hand-side state (identical in all blocks).
+struct RhsState {
+  double alpha[PCG_MAX_RHS], beta[PCG_MAX_RHS], rz[PCG_MAX_RHS], rzold[PCG_MAX_RHS];
+  double rr[PCG_MAX_RHS], res[PCG_MAX_RHS], resmax[PCG_MAX_RHS];
+  int iters[PCG_MAX_RHS], lastru[PCG_MAX_RHS], status[PCG_MAX_RHS];
+  unsigned char active[PCG_MAX_RHS], ru[PCG_MAX_RHS];
+  int any_active, any_ru;
+  double red[32];
+};
+
+// ---------------------------------------------------------------------------
+// the persistent kernel
+// ---------------------------------------------------------------------------
+template <typename RS, typename RH, typename A, int BY, bool PHS_S, bool PHS_H>
+__global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_constant__ PcgParams p) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ RhsState st;
+  constexpr bool MIXED = !std::is_same<RS, RH>::value;
+  const int NV = p.nrhs;
+  Acc acc(p.acc, NV);
+  const unsigned int nblk = gridDim.x;
+  const int tid = threadIdx.x;
+  const RS* zbuf = reinterpret_cast<const RS*>(p.z);
+  RS* r = reinterpret_cast<RS*>(p.r);
+  RS* z = reinterpret_cast<RS*>(p.z);
+  RS* Op = reinterpret_cast<RS*>(p.Op);
+  RS* xs = MIXED ? reinterpret_cast<RS*>(p.xlo) : reinterpret_cast<RS*>(p.x);
+  RH* xh = reinterpret_cast<RH*>(p.x);
+  const RH* bvec = reinterpret_cast<const RH*>(p.b);
+  const A* phi_all = reinterpret_cast<const A*>(p.phi);
+  const int CH = p.CH;
+
+  for (int v = tid; v < NV; v += blockDim.x) {
+    st.active[v] = 1;
+    st.iters[v] = 0;
+    st.lastru[v] = 0;
+    st.status[v] = QEDF_OK;
+    st.resmax[v] = 1.0;
+    st.ru[v] = 0;
+  }
+  __syncthreads();
+
+  // elementwise unit decode
+  auto unitE = [&](int u, int& s, int& v, int& c0, int& c1) {
+    s = find_sys_E(p, u);
+    const PcgSys& S = p.sys[s];
+    const int lu = u - S.unitE0;
+    v = S.rhs0 + lu / S.nchunk;
+    const int Vs = S.L * S.L;
+    c0 = (lu % S.nchunk) * CH;
+    c1 = min(c0 + CH, Vs);
+  };
+  auto vec_base = [&](int s, int v) -> int64_t {
+    const PcgSys& S = p.sys[s];
+    return S.vec0 + (int64_t)(v - S.rhs0) * S.Nt * S.L * S.L;
+  };
+
+  // ---- BC-type elementwise pass over one unit --------------------------------
+  // kind 0: init (x = 0, r = b, bb); 1: iteration update; 2: preconditioner only
+  // (after a reliable update).  Leaves r of the chunk in smem, applies P.
+  auto elementwise = [&](int kind, int u, int slot) {
+    int s, v, c0, c1;
+    unitE(u, s, v, c0, c1);
+    const PcgSys& S = p.sys[s];
+    const int Vs = S.L * S.L, Nt = S.Nt, w = c1 - c0;
+    const int64_t base = vec_base(s, v);
+    Cx<RS>* rsm = reinterpret_cast<Cx<RS>*>(dsm);
+    const RS al = (RS)st.alpha[v];
+    const RS* pn = reinterpret_cast<const RS*>((st.iters[v] & 1) ? p.p1 : p.p0);
+    double acc_a = 0, acc_b = 0;
+    for (int e = tid; e < Nt * CH; e += blockDim.x) {
+      const int t = e / CH, j = e % CH;
+      if (j >= w) continue;
+      const int64_t i = base + (int64_t)t * Vs + c0 + j;
+      Cx<RS> rv;
+      if (kind == 0) {
+        const Cx<RH> bv = ldc(bvec, i);
+        acc_a += (double)bv.re * bv.re + (double)bv.im * bv.im;  // bb
+        rv = mk<RS>((RS)bv.re, (RS)bv.im);
+        stc(xs, i, mk<RS>(0, 0));
+        if (MIXED) stc(xh, i, mk<RH>(0, 0));
+        stc(r, i, rv);
+      } else if (kind == 1) {
+        const Cx<RS> pv = ldc(pn, i), ov = ldc(reinterpret_cast<const RS*>(Op), i);
+        Cx<RS> xv = ldc(reinterpret_cast<const RS*>(xs), i);
+        rv = ldc(reinterpret_cast<const RS*>(r), i);
+        xv = mk<RS>(fma(al, pv.re, xv.re), fma(al, pv.im, xv.im));
+        rv = mk<RS>(fma(-al, ov.re, rv.re), fma(-al, ov.im, rv.im));
+        stc(xs, i, xv);
+        stc(r, i, rv);
+      } else {
+        rv = ldc(reinterpret_cast<const RS*>(r), i);
+      }
+      if (kind != 0) acc_a += (double)rv.re * rv.re + (double)rv.im * rv.im;  // rr
+      rsm[t * CH + j] = rv;
+    }
+    __syncthreads();
+    for (int e = tid; e < Nt * CH; e += blockDim.x) {
+      const int t = e / CH, j = e % CH;
+      if (j >= w) continue;
+      const int64_t i = base + (int64_t)t * Vs + c0 + j;
+      const Cx<RS> rv = rsm[t * CH + j];
+      Cx<RS> zv;
+      if (S.precon) {
+        RS zr = 0, zi = 0;
+        pre_row(c_pre, Nt, t, [&](int col, float val) {
+          const Cx<RS> q = rsm[col * CH + j];
+          zr = fma((RS)val, q.re, zr);
+          zi = fma((RS)val, q.im, zi);
+        });
+        zv = mk<RS>(zr, zi);
+        stc(z, i, zv);
+      } else {
+        zv = rv;
+      }
+      acc_b += (double)rv.re * zv.re + (double)rv.im * zv.im;  // rz
+    }
+    // rr for init equals bb (r = b): accumulate separately
+    double rr_init = 0;
+    if (kind == 0) {
+      for (int e = tid; e < Nt * CH; e += blockDim.x) {
+        const int j = e % CH;
+        if (j >= w) continue;
+        const Cx<RS> q = rsm[e];
+        rr_init += (double)q.re * q.re + (double)q.im * q.im;
+      }
+    }
+    const double sa = block_sum_d(acc_a, st.red);
+    const double sb = block_sum_d(acc_b, st.red);
+    const double sc = block_sum_d(rr_init, st.red);
+    if (tid == 0) {
+      if (kind == 0) {
+        atomicAdd(acc.bb + v, sa);
+        atomicAdd(acc.rr + slot * NV + v, sc);
+        atomicAdd(acc.rz + slot * NV + v, sb);
+      } else if (kind == 1) {
+        atomicAdd(acc.rr + slot * NV + v, sa);
+        atomicAdd(acc.rz + slot * NV + v, sb);
+      } else {
+        atomicAdd(acc.ru_rz + v, sb);
+      }
+    }
+    __syncthreads();
+  };
+
+  // ---- operator pass over one unit -------------------------------------------
+  // p_new = z + beta p_old on the slab and its halo slices, Op = M^dag M p_new,
+  // and pAp = p_new^dag M^dag M p_new = sum_t |(M p_new)_t|^2 over the slab.
+  auto operator_unit_sloppy = [&](int u, int slot) {
+    const int s = find_sys_A(p, u);
+    const PcgSys& S = p.sys[s];
+    const int lu = u - S.unitA0;
+    const int v = S.rhs0 + lu / S.nslab;
+    const int a = (lu % S.nslab) * S.T;
+    const int bnd = min(a + S.T, S.Nt);
+    const int Nt = S.Nt, Vs = S.L * S.L;
+    const size_t sv = 2 * (size_t)Vs;
+    Slice<RS, BY, PHS_S> E;
+    E.init(S.L, dsm, 2, (RS)p.c1, (RS)p.ch, tid);
+    const int64_t vb = 2 * vec_base(s, v);  // reals
+    const A* phi = phi_all + S.phi0 + (S.shared ? 0 : (int64_t)(v - S.rhs0) * Nt * sv);
+    const RS beta = (RS)st.beta[v];
+    const bool has_old = st.iters[v] > 0;
+    const RS* pold = reinterpret_cast<const RS*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
+    RS* pnew = reinterpret_cast<RS*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
+    const RS* zz = (S.precon ? zbuf : reinterpret_cast<const RS*>(r)) + vb;
+    RS* O = Op + vb;
+    const RS t1 = (RS)p.t1, th = (RS)p.th, Cb = (RS)p.Cb;
+    Cx<RS> X0[BY][2], X1[BY][2], Y[BY][2];
+    double pap = 0;
+    auto getp = [&](Cx<RS> (&X)[BY][2], int t) {
+      if (!E.on) return;
+      E.load_coherent(X, zz + t * sv);
+      if (has_old) {
+        Cx<RS> T0[BY][2];
+        E.load_coherent(T0, pold + t * sv);
+#pragma unroll
+        for (int q = 0; q < BY; ++q)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            X[q][c].re = fma(beta, T0[q][c].re, X[q][c].re);
+            X[q][c].im = fma(beta, T0[q][c].im, X[q][c].im);
+          }
+      }
+    };
+    const int tp = (a - 1 + Nt) % Nt;
+    getp(X0, tp);
+    getp(X1, a);
+    if (E.on) E.store(pnew + a * sv, X1);
+    E.phases(phi + tp * sv, t1, th);
+    E.template applyB<FAC_TILDE>(X0);
+    axpy_blk<RS, BY>(Y, X1, sigma_of<RS>(tp, Nt) * Cb, X0);  // y_a
+    E.park(Y);
+    copy_blk<RS, BY>(X0, X1);
+    for (int t = a; t < bnd; ++t) {
+      const int tn = (t + 1) % Nt;
+      getp(X1, tn);
+      if (E.on && t + 1 < bnd) E.store(pnew + tn * sv, X1);
+      E.phases(phi + t * sv, t1, th);
+      const RS sg = sigma_of<RS>(t, Nt) * Cb;
+      E.template applyB<FAC_TILDE>(X0);       // B_t p_t
+      axpy_blk<RS, BY>(Y, X1, sg, X0);         // y_{t+1}
+      E.unpark(X0);                            // y_t
+      E.park(Y);
+      if (E.on) {
+#pragma unroll
+        for (int q = 0; q < BY; ++q)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) pap += (double)X0[q][c].re * X0[q][c].re + (double)X0[q][c].im * X0[q][c].im;
+      }
+      E.template applyB<FAC_TILDE>(Y);        // B_t y_{t+1}
+      if (E.on) {
+        axpy_blk<RS, BY>(Y, X0, sg, Y);        // (M^dag M p)_t
+        E.store(O + t * sv, Y);
+      }
+      copy_blk<RS, BY>(X0, X1);
+    }
+    const double sum = block_sum_d(pap, st.red);
+    if (tid == 0) atomicAdd(acc.pAp + slot * NV + v, sum);
+    __syncthreads();
+  };
+
+  // r = b - M^dag M x in the high precision (mixed mode), rr_true
+  auto operator_unit_true_residual = [&](int u) {
+    const int s = find_sys_A(p, u);
+    const PcgSys& S = p.sys[s];
+    const int lu = u - S.unitA0;
+    const int v = S.rhs0 + lu / S.nslab;
+    const int a = (lu % S.nslab) * S.T;
+    const int bnd = min(a + S.T, S.Nt);
+    const int Nt = S.Nt, Vs = S.L * S.L;
+    const size_t sv = 2 * (size_t)Vs;
+    Slice<RH, BY, PHS_H> E;
+    E.init(S.L, dsm, 2, (RH)p.c1, (RH)p.ch, tid);
+    const int64_t vb = 2 * vec_base(s, v);
+    const A* phi = phi_all + S.phi0 + (S.shared ? 0 : (int64_t)(v - S.rhs0) * Nt * sv);
+    const RH* xx = xh + vb;
+    const RH* bb = bvec + vb;
+    RS* rout = r + vb;
+    const RH t1 = (RH)p.t1, th = (RH)p.th, Cb = (RH)p.Cb;
+    Cx<RH> X0[BY][2], X1[BY][2], Y[BY][2];
+    double rr_acc = 0;
+    const int tp = (a - 1 + Nt) % Nt;
+    if (E.on) {
+      E.load_coherent(X0, xx + tp * sv);
+      E.load_coherent(X1, xx + a * sv);
+    }
+    E.phases(phi + tp * sv, t1, th);
+    E.template applyB<FAC_TILDE>(X0);
+    axpy_blk<RH, BY>(Y, X1, sigma_of<RH>(tp, Nt) * Cb, X0);
+    E.park(Y);
+    copy_blk<RH, BY>(X0, X1);
+    for (int t = a; t < bnd; ++t) {
+      const int tn = (t + 1) % Nt;
+      if (E.on) E.load_coherent(X1, xx + tn * sv);
+      E.phases(phi + t * sv, t1, th);
+      const RH sg = sigma_of<RH>(t, Nt) * Cb;
+      E.template applyB<FAC_TILDE>(X0);
+      axpy_blk<RH, BY>(Y, X1, sg, X0);
+      E.unpark(X0);
+      E.park(Y);
+      E.template applyB<FAC_TILDE>(Y);
+      if (E.on) {
+        axpy_blk<RH, BY>(Y, X0, sg, Y);  // (A x)_t
+        E.load_coherent(X0, bb + t * sv);
+#pragma unroll
+        for (int q = 0; q < BY; ++q)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            const RH dr = X0[q][c].re - Y[q][c].re, di = X0[q][c].im - Y[q][c].im;
+            rr_acc += (double)dr * dr + (double)di * di;
+            const int64_t site = (int64_t)t * Vs + (E.y0 + q) * S.L + E.x0 + c;
+            rout[2 * site] = (RS)dr;
+            rout[2 * site + 1] = (RS)di;
+          }
+      }
+      copy_blk<RH, BY>(X0, X1);
+    }
+    const double sum = block_sum_d(rr_acc, st.red);
+    if (tid == 0) atomicAdd(acc.ru_rr + v, sum);
+    __syncthreads();
+  };
+
+  // x (double) += x_lo; x_lo = 0   for the flagged right-hand sides
+  auto fold_unit = [&](int u, bool all_active) {
+    int s, v, c0, c1;
+    unitE(u, s, v, c0, c1);
+    if (!(all_active ? st.active[v] : st.ru[v])) return;
+    const PcgSys& S = p.sys[s];
+    const int Vs = S.L * S.L, w = c1 - c0;
+    const int64_t base = vec_base(s, v);
+    for (int e = tid; e < S.Nt * CH; e += blockDim.x) {
+      const int t = e / CH, j = e % CH;
+      if (j >= w) continue;
+      const int64_t i = base + (int64_t)t * Vs + c0 + j;
+      const Cx<RS> lo = ldc(reinterpret_cast<const RS*>(xs), i);
+      Cx<RH> hi = ldc(reinterpret_cast<const RH*>(xh), i);
+      hi.re += (RH)lo.re;
+      hi.im += (RH)lo.im;
+      stc(xh, i, hi);
+      stc(xs, i, mk<RS>(0, 0));
+    }
+  };
+
+  // ---------------------------------------------------------------------------
+  const long long budget = p.timeout_cycles;
+  bool ok = true;
+
+  // init: x = 0, r = b, z = P r
+  for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) elementwise(0, u, 0);
+  ok = grid_barrier(p.bar, nblk, budget);
+  int slot = 0;  // accumulator slot holding the current rr / rz
+  if (ok) {
+    for (int v = tid; v < NV; v += blockDim.x) {
+      st.rz[v] = acc.rz[v];
+      st.rzold[v] = 1.0;
+      st.rr[v] = acc.rr[v];
+      const double bbv = acc.bb[v];
+      if (bbv == 0.0) {  // b = 0: x = 0 is exact
+        st.active[v] = 0;
+        st.res[v] = 0.0;
+      }
+    }
+    __syncthreads();
+  }
+
+  int it = 0;
+  while (ok) {
+    // ---- convergence / reliable-update decisions (identical in every block)
+    if (tid == 0) {
+      st.any_ru = 0;
+      st.any_active = 0;
+    }
+    __syncthreads();
+    for (int v = tid; v < NV; v += blockDim.x) {
+      st.ru[v] = 0;
+      if (!st.active[v]) continue;
+      const double bbv = acc.bb[v];
+      const double res = sqrt(st.rr[v] / bbv);
+      st.res[v] = res;
+      if (!isfinite(res)) {
+        st.active[v] = 0;
+        st.status[v] = QEDF_ERR_NAN;
+        continue;
+      }
+      if (MIXED) {
+        if (res <= p.rtol || it - st.lastru[v] >= p.ru_interval || res < p.ru_delta * st.resmax[v]) {
+          st.ru[v] = 1;
+          st.any_ru = 1;
+        }
+      } else if (res <= p.rtol) {
+        st.active[v] = 0;
+      }
+    }
+    __syncthreads();
+    if (MIXED && st.any_ru) {
+      if (blockIdx.x == 0)
+        for (int v = tid; v < NV; v += blockDim.x) {
+          acc.ru_rr[v] = 0;
+          acc.ru_rz[v] = 0;
+        }
+      for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) fold_unit(u, false);
+      if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+      for (int u = blockIdx.x; u < p.unitsA; u += gridDim.x) {
+        const int s = find_sys_A(p, u);
+        const int v = p.sys[s].rhs0 + (u - p.sys[s].unitA0) / p.sys[s].nslab;
+        if (st.ru[v]) operator_unit_true_residual(u);
+      }
+      if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+      for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) {
+        int s, v, c0, c1;
+        unitE(u, s, v, c0, c1);
+        if (st.ru[v]) elementwise(2, u, 0);
+      }
+      if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+      for (int v = tid; v < NV; v += blockDim.x) {
+        if (!st.ru[v]) continue;
+        st.rr[v] = acc.ru_rr[v];
+        st.rz[v] = acc.ru_rz[v];
+        const double res = sqrt(st.rr[v] / acc.bb[v]);
+        st.res[v] = res;
+        st.resmax[v] = res;
+        st.lastru[v] = it;
+        if (!isfinite(res)) {
+          st.active[v] = 0;
+          st.status[v] = QEDF_ERR_NAN;
+        } else if (res <= p.rtol) {
+          st.active[v] = 0;
+        }
+      }
+      __syncthreads();
+    }
+    for (int v = tid; v < NV; v += blockDim.x)
+      if (st.active[v]) st.any_active = 1;
+    __syncthreads();
+    if (!st.any_active || it >= p.max_iter) break;
+
+    // ---- phase A
+    for (int v = tid; v < NV; v += blockDim.x) st.beta[v] = st.iters[v] > 0 ? st.rz[v] / st.rzold[v] : 0.0;
+    __syncthreads();
+    const int aslot = it & 1;
+    for (int u = blockIdx.x; u < p.unitsA; u += gridDim.x) {
+      const int s = find_sys_A(p, u);
+      const int v = p.sys[s].rhs0 + (u - p.sys[s].unitA0) / p.sys[s].nslab;
+      if (st.active[v]) operator_unit_sloppy(u, aslot);
+    }
+    // the rr/rz slot that BC will fill was last read before the previous barrier
+    if (blockIdx.x == 0)
+      for (int v = tid; v < NV; v += blockDim.x) {
+        acc.rr[(slot ^ 1) * NV + v] = 0;
+        acc.rz[(slot ^ 1) * NV + v] = 0;
+      }
+    if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+
+    // ---- phase BC
+    for (int v = tid; v < NV; v += blockDim.x) st.alpha[v] = st.rz[v] / acc.pAp[aslot * NV + v];
+    __syncthreads();
+    for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) {
+      int s, v, c0, c1;
+      unitE(u, s, v, c0, c1);
+      if (st.active[v]) elementwise(1, u, slot ^ 1);
+    }
+    if (blockIdx.x == 0)  // pAp slot of the next iteration
+      for (int v = tid; v < NV; v += blockDim.x) acc.pAp[(aslot ^ 1) * NV + v] = 0;
+    if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+    slot ^= 1;
+    for (int v = tid; v < NV; v += blockDim.x) {
+      if (!st.active[v]) continue;
+      st.rzold[v] = st.rz[v];
+      st.rz[v] = acc.rz[slot * NV + v];
+      st.rr[v] = acc.rr[slot * NV + v];
+      st.iters[v] += 1;
+    }
+    __syncthreads();
+    ++it;
+  }
+
+  // mixed: fold the remaining float updates of unconverged systems into x
+  if (MIXED && ok) {
+    for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) fold_unit(u, true);
+  }
+  if (blockIdx.x == 0) {
+    const unsigned int err = *((volatile unsigned int*)(p.bar + 2));
+    for (int v = tid; v < NV; v += blockDim.x) {
+      int stt = st.status[v];
+      if (err) stt = (int)err;
+      else if (stt == QEDF_OK && st.active[v]) stt = QEDF_ERR_MAXITER;
+      p.status[v] = stt;
+      p.iters[v] = st.iters[v];
+      p.relres[v] = st.res[v];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts* o) {
+  std::memset(&p, 0, sizeof(p));
+  if (!sys || !o || nsys <= 0 || nsys > PCG_MAX_SYS) return QEDF_ERR_ARG;
+  if (o->mode != QEDF_PCG_PLAIN_F32 && o->mode != QEDF_PCG_PLAIN_F64 && o->mode != QEDF_PCG_MIXED)
+    return QEDF_ERR_ARG;
+  p.mode = o->mode;
+  p.nsys = nsys;
+  p.CH = o->chunk > 0 ? o->chunk : 16;
+  const int nblk = num_sms();
+  int rhs = 0, ua = 0, ue = 0;
+  int64_t vec = 0, phi = 0;
+  for (int s = 0; s < nsys; ++s) {
+    const qedf_system& q = sys[s];
+    if (q.Lx < 2 || q.Lx % 2 || q.Ltau < 2 || q.nrhs < 1) return QEDF_ERR_ARG;
+    PcgSys& S = p.sys[s];
+    S.L = q.Lx;
+    S.Nt = q.Ltau;
+    S.nrhs = q.nrhs;
+    S.shared = q.shared_boson ? 1 : 0;
+    S.precon = (o->use_precon && q.Ltau >= PRE_MIN_LTAU) ? 1 : 0;
+    if (o->slab > 0) {
+      S.T = o->slab;
+    } else {
+      // about one operator unit per block over all right-hand sides
+      int total_rhs = 0;
+      for (int k = 0; k < nsys; ++k) total_rhs += sys[k].nrhs;
+      const int per_rhs = std::max(1, nblk / std::max(1, total_rhs));
+      S.T = std::max(1, (q.Ltau + per_rhs - 1) / per_rhs);
+    }
+    S.nslab = (q.Ltau + S.T - 1) / S.T;
+    S.nchunk = (q.Lx * q.Lx + p.CH - 1) / p.CH;
+    S.rhs0 = rhs;
+    S.unitA0 = ua;
+    S.unitE0 = ue;
+    S.vec0 = vec;
+    S.phi0 = phi;
+    rhs += q.nrhs;
+    ua += q.nrhs * S.nslab;
+    ue += q.nrhs * S.nchunk;
+    vec += (int64_t)q.nrhs * q.Ltau * q.Lx * q.Lx;
+    phi += (int64_t)(S.shared ? 1 : q.nrhs) * q.Ltau * q.Lx * q.Lx * 2;
+  }
+  if (rhs > PCG_MAX_RHS) return QEDF_ERR_SIZE;
+  p.nrhs = rhs;
+  p.unitsA = ua;
+  p.unitsE = ue;
+  p.nvec_total = vec;
+  p.max_iter = o->max_iter;
+  p.rtol = o->rtol;
+  p.ru_interval = o->ru_interval > 0 ? o->ru_interval : 50;
+  p.ru_delta = o->ru_delta > 0 ? o->ru_delta : 0.1;
+  const FactorCoeffs f = factor_coeffs(o->dtau);
+  p.c1 = f.c1;
+  p.ch = f.ch;
+  p.t1 = f.t1;
+  p.th = f.th;
+  p.Cb = f.Cb;
+  return QEDF_OK;
+}
+
+size_t pcg_workspace_bytes(const PcgParams& p, int sloppy_bytes) {
+  const size_t vecb = align_up((size_t)p.nvec_total * 2 * sloppy_bytes, 256);
+  const int nv = p.mode == QEDF_PCG_MIXED ? 6 : 5;
+  const size_t accb = align_up(sizeof(double) * ACC_PER_RHS * p.nrhs, 256);
+  return nv * vecb + accb + 256;
+}
+
+template <typename RS, typename RH, typename A, int BY, bool PHS_S, bool PHS_H>
+static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
+  int Lmax = 0, Ntmax = 0;
+  for (int s = 0; s < p.nsys; ++s) {
+    Lmax = std::max(Lmax, p.sys[s].L);
+    Ntmax = std::max(Ntmax, p.sys[s].Nt);
+    if (p.sys[s].L % BY) return QEDF_ERR_ARG;
+  }
+  const int eng_threads = (Lmax / 2) * (Lmax / BY);
+  if (eng_threads > MaxThreads<BY>::value) return QEDF_ERR_SIZE;
+  const int threads = std::min(MaxThreads<BY>::value, std::max(128, (eng_threads + 31) / 32 * 32));
+  size_t smem = slice_smem_bytes<RS, PHS_S>(Lmax, BY, 2);
+  smem = std::max(smem, slice_smem_bytes<RH, PHS_H>(Lmax, BY, 2));
+  smem = std::max(smem, sizeof(Cx<RS>) * (size_t)Ntmax * p.CH);
+  if (smem + sizeof(RhsState) > 227 * 1024) return QEDF_ERR_SIZE;
+  auto kern = k_pcg<RS, RH, A, BY, PHS_S, PHS_H>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return QEDF_ERR_CUDA;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+    return QEDF_ERR_SIZE;
+  const int nblk = num_sms() * per_sm;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nblk);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, kern, p) != cudaSuccess) return QEDF_ERR_CUDA;
+  return QEDF_OK;
+}
+
+static size_t pcg_fixed_smem(const PcgParams& p, int real_bytes, int& Lmax) {
+  int Ntmax = 0;
+  Lmax = 0;
+  for (int s = 0; s < p.nsys; ++s) {
+    Lmax = std::max(Lmax, p.sys[s].L);
+    Ntmax = std::max(Ntmax, p.sys[s].Nt);
+  }
+  return (size_t)real_bytes * 2 * Ntmax * p.CH + sizeof(RhsState);
+}
+
+template <int BY>
+static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
+  int Lmax = 0;
+  switch (p.mode) {
+    case QEDF_PCG_PLAIN_F32: return launch_pcg_t<float, float, float, BY, false, false>(p, st);
+    case QEDF_PCG_PLAIN_F64: {
+      pcg_fixed_smem(p, 8, Lmax);
+      if (slice_smem_bytes<double, true>(Lmax, BY, 2) + sizeof(RhsState) <= 227 * 1024)
+        return launch_pcg_t<double, double, double, BY, true, true>(p, st);
+      return launch_pcg_t<double, double, double, BY, false, false>(p, st);
+    }
+    case QEDF_PCG_MIXED: {
+      pcg_fixed_smem(p, 4, Lmax);
+      if (slice_smem_bytes<double, true>(Lmax, BY, 2) + sizeof(RhsState) <= 227 * 1024)
+        return launch_pcg_t<float, double, float, BY, false, true>(p, st);
+      return launch_pcg_t<float, double, float, BY, false, false>(p, st);
+    }
+  }
+  return QEDF_ERR_ARG;
+}
+
+int launch_pcg(PcgParams& p, int by, cudaStream_t st) {
+  if (by <= 0) {
+    // the tile must divide every system's L; prefer the smallest that fits
+    int Lmax = 0;
+    for (int s = 0; s < p.nsys; ++s) Lmax = std::max(Lmax, p.sys[s].L);
+    const int wide = p.mode == QEDF_PCG_PLAIN_F32 ? 2 : 4;
+    const int order[3] = {wide, wide == 2 ? 4 : 2, 6};
+    by = -1;
+    for (int c : order) {
+      bool ok = (Lmax / 2) * (Lmax / c) <= (c == 2 ? MaxThreads<2>::value : c == 4 ? MaxThreads<4>::value
+                                                                                 : MaxThreads<6>::value);
+      for (int s = 0; s < p.nsys; ++s) ok = ok && p.sys[s].L % c == 0;
+      if (ok) {
+        by = c;
+        break;
+      }
+    }
+    if (by < 0) return QEDF_ERR_SIZE;
+  }
+  switch (by) {
+    case 2: return launch_pcg_by<2>(p, st);
+    case 4: return launch_pcg_by<4>(p, st);
+    case 6: return launch_pcg_by<6>(p, st);
+  }
+  return QEDF_ERR_ARG;
+}
+
+}  // namespace qedf
+
+extern "C" int qedf_precon_tau_csr(int Ltau, int* row_ptr, int* col, double* val, int* nnz) {
+  using namespace qedf;
+  if (Ltau < PRE_MIN_LTAU || !row_ptr || !nnz) return QEDF_ERR_ARG;
+  int k = 0;
+  for (int t = 0; t < Ltau; ++t) {
+    row_ptr[t] = k;
+    // collect and sort the row by column
+    int cols[32];
+    double vals[32];
+    int n = 0;
+    pre_row(h_pre, Ltau, t, [&](int c, float v) {
+      cols[n] = c;
+      vals[n] = (double)v;
+      ++n;
+    });
+    for (int i = 1; i < n; ++i)
+      for (int j = i; j > 0 && cols[j - 1] > cols[j]; --j) {
+        std::swap(cols[j - 1], cols[j]);
+        std::swap(vals[j - 1], vals[j]);
+      }
+    for (int i = 0; i < n; ++i, ++k)
+      if (col && val) {
+        col[k] = cols[i];
+        val[k] = vals[i];
+      }
+  }
+  row_ptr[Ltau] = k;
+  *nnz = k;
+  return QEDF_OK;
+}

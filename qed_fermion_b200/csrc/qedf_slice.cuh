@@ -1,0 +1,311 @@
+// Slice engine: applies the checkerboard bond factors of one imaginary-time
+// slice to a vector held in registers by one thread block.
+//
+// Thread mapping.  The L x L slice is tiled by 2 x BY site blocks; thread
+// (bx, by) owns x in {2bx, 2bx+1} and y in [BY*by, BY*by + BY).  Because x0
+// and y0 are even, every bond factor pairs sites either inside the block
+// ("local") or across its edge with the neighbouring block ("cross"):
+//
+//   g1 (x-bond A -> A+x):  local in even rows, cross in odd rows
+//   g3 (x-bond A-x -> A):  local in odd rows,  cross in even rows
+//   g2 (y-bond A -> A+y):  local in column x0, cross at the ends of x0+1
+//   g4 (y-bond A-y -> A):  local in column x0+1, cross at the ends of x0
+//
+// (A = sites with x = y mod 2, the ordering of the reference's
+// initialize_geometry, hmc_sampler_batch.py:937-969).  A factor application
+// exports the values that neighbours need into a shared-memory buffer,
+// synchronises once, and updates every owned site from its old value and its
+// partner's old value.  Two exchange buffers alternate, so one barrier per
+// factor is enough.  The bond phases t_g e^{i phi} of a slice are computed
+// once by the owner of the bond's origin site and kept in registers; the
+// phases a thread needs from its left and upper neighbours go through shared
+// memory once per slice.
+#pragma once
+
+#include "qedf_common.cuh"
+
+namespace qedf {
+
+enum FacMode { FAC_TILDE = 0, FAC_TRUE = 1, FAC_INV = 2 };
+
+// Largest thread block each tile height is compiled for (it fixes the
+// register budget: 65536 / MAXT registers per thread).
+template <int BY>
+struct MaxThreads {
+  static constexpr int value = BY == 2 ? 576 : (BY == 4 ? 512 : 384);
+};
+
+// Shared-memory size (bytes) of one slice engine: nbuf exchange buffers, the
+// phase tables and a thread-private stash of one vector.  PHS = false keeps a
+// thread's own bond phases in registers and only the neighbours' in shared
+// memory; PHS = true (used in double precision to relieve registers) keeps
+// the phases of all 2 Vs bonds of the slice in shared memory.
+template <typename R, bool PHS = false>
+__host__ __device__ inline size_t slice_smem_bytes(int L, int BY, int nbuf) {
+  const size_t Vs = (size_t)L * L;
+  const size_t ph = PHS ? 2 * Vs : Vs / 2 + Vs / BY;
+  return sizeof(Cx<R>) * (nbuf * Vs + ph + Vs);
+}
+
+template <typename R, int BY, bool PHS = false>
+struct Slice {
+  static_assert(BY % 2 == 0, "BY must be even");
+  int L, nbx, nby, bx, by, x0, y0, bxl, bxr, byu, byd;
+  bool on;
+  Cx<R>* xb[4];  // exchange buffers (Vs complex each)
+  Cx<R>* phr;    // PHS: [2 Vs] all bond phases;  else [L][nbx] x-bond phases of column x0+1
+  Cx<R>* phb;    // (register mode) [nby][L] y-bond phases of the last row of every block
+  Cx<R>* stash;  // [Vs]       each thread parks its own block of one vector here
+  int cur;
+  R c1, ch;      // cosh(dtau), cosh(dtau/2)
+  Cx<R> tpx_[PHS ? 1 : BY][2], tpy_[PHS ? 1 : BY][2], tpl_[PHS ? 1 : BY], tpt_[2];
+
+  // phase of the x-bond / y-bond starting at own site (x0+c, y0+r), of the
+  // x-bond arriving from the left in row r, of the y-bond arriving from above
+  __device__ __forceinline__ Cx<R> TPX(int r, int c) const {
+    return PHS ? phr[2 * ((y0 + r) * L + x0 + c)] : tpx_[PHS ? 0 : r][c];
+  }
+  __device__ __forceinline__ Cx<R> TPY(int r, int c) const {
+    return PHS ? phr[2 * ((y0 + r) * L + x0 + c) + 1] : tpy_[PHS ? 0 : r][c];
+  }
+  __device__ __forceinline__ Cx<R> TPL(int r) const {
+    return PHS ? phr[2 * ((y0 + r) * L + (x0 + L - 1) % L)] : tpl_[PHS ? 0 : r];
+  }
+  __device__ __forceinline__ Cx<R> TPT(int c) const {
+    return PHS ? phr[2 * (((y0 + L - 1) % L) * L + x0 + c) + 1] : tpt_[c];
+  }
+
+  // smem must hold slice_smem_bytes<R, PHS>(L, BY, nbuf)
+  __device__ void init(int L_, unsigned char* smem, int nbuf, R c1_, R ch_, int tid) {
+    L = L_;
+    nbx = L / 2;
+    nby = L / BY;
+    on = tid < nbx * nby;
+    bx = on ? tid % nbx : 0;
+    by = on ? tid / nbx : 0;
+    x0 = 2 * bx;
+    y0 = BY * by;
+    bxl = (bx + nbx - 1) % nbx;
+    bxr = (bx + 1) % nbx;
+    byu = (by + nby - 1) % nby;
+    byd = (by + 1) % nby;
+    const int Vs = L * L;
+    Cx<R>* base = reinterpret_cast<Cx<R>*>(smem);
+    for (int i = 0; i < 4; ++i) xb[i] = base + (size_t)(i < nbuf ? i : 0) * Vs;
+    phr = base + (size_t)nbuf * Vs;
+    phb = phr + Vs / 2;
+    stash = PHS ? phr + 2 * Vs : phb + Vs / BY;
+    cur = 0;
+    c1 = c1_;
+    ch = ch_;
+  }
+
+  // ---- global memory ------------------------------------------------------
+  // slice: complex vector of the slice (2*Vs reals)
+  __device__ __forceinline__ void load(Cx<R> (&v)[BY][2], const R* slice) const {
+#pragma unroll
+    for (int r = 0; r < BY; ++r) ld2(slice + 2 * ((y0 + r) * L + x0), v[r][0], v[r][1]);
+  }
+  __device__ __forceinline__ void load_coherent(Cx<R> (&v)[BY][2], const R* slice) const {
+#pragma unroll
+    for (int r = 0; r < BY; ++r) ld2c(slice + 2 * ((y0 + r) * L + x0), v[r][0], v[r][1]);
+  }
+  __device__ __forceinline__ void store(R* slice, const Cx<R> (&v)[BY][2]) const {
+#pragma unroll
+    for (int r = 0; r < BY; ++r) st2(slice + 2 * ((y0 + r) * L + x0), v[r][0], v[r][1]);
+  }
+
+  // thread-private parking of one block (no synchronisation needed)
+  __device__ __forceinline__ void park(const Cx<R> (&v)[BY][2]) const {
+    if (!on) return;
+#pragma unroll
+    for (int r = 0; r < BY; ++r) {
+      stash[(y0 + r) * L + x0] = v[r][0];
+      stash[(y0 + r) * L + x0 + 1] = v[r][1];
+    }
+  }
+  __device__ __forceinline__ void unpark(Cx<R> (&v)[BY][2]) const {
+    if (!on) return;
+#pragma unroll
+    for (int r = 0; r < BY; ++r) {
+      v[r][0] = stash[(y0 + r) * L + x0];
+      v[r][1] = stash[(y0 + r) * L + x0 + 1];
+    }
+  }
+
+  // ---- bond phases of one slice --------------------------------------------
+  // ang: the slice's 2*Vs angles (A = float or double); t1 = tanh(dtau),
+  // th = tanh(dtau/2).  Contains one __syncthreads().
+  template <typename A>
+  __device__ void phases(const A* ang, R t1, R th) {
+    if (PHS) {
+      if (on) {
+#pragma unroll
+        for (int r = 0; r < BY; ++r) {
+          A a[4];
+          ld4(ang + 2 * ((y0 + r) * L + x0), a);
+          Cx<R>* q = phr + 2 * ((y0 + r) * L + x0);
+          // x-bond of (x0+c, y0+r) is in g1 when the site is an A site, else g3
+          q[0] = tphase((R)a[0], (r & 1) == 0 ? t1 : th);
+          q[1] = tphase((R)a[1], th);
+          q[2] = tphase((R)a[2], (r & 1) == 1 ? t1 : th);
+          q[3] = tphase((R)a[3], th);
+        }
+      }
+      __syncthreads();
+      return;
+    }
+    if (on) {
+#pragma unroll
+      for (int r = 0; r < BY; ++r) {
+        A a[4];
+        ld4(ang + 2 * ((y0 + r) * L + x0), a);
+        // x-bond of (x0+c, y0+r) is in g1 when the site is an A site, else g3
+        tpx_[PHS ? 0 : r][0] = tphase((R)a[0], (r & 1) == 0 ? t1 : th);
+        tpy_[PHS ? 0 : r][0] = tphase((R)a[1], th);
+        tpx_[PHS ? 0 : r][1] = tphase((R)a[2], (r & 1) == 1 ? t1 : th);
+        tpy_[PHS ? 0 : r][1] = tphase((R)a[3], th);
+      }
+#pragma unroll
+      for (int r = 0; r < BY; ++r) phr[(y0 + r) * nbx + bx] = tpx_[PHS ? 0 : r][1];
+      phb[by * L + x0] = tpy_[PHS ? 0 : BY - 1][0];
+      phb[by * L + x0 + 1] = tpy_[PHS ? 0 : BY - 1][1];
+    }
+    __syncthreads();
+    if (on) {
+#pragma unroll
+      for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = phr[(y0 + r) * nbx + bxl];
+      tpt_[0] = phb[byu * L + x0];
+      tpt_[1] = phb[byu * L + x0 + 1];
+    }
+  }
+
+  // ---- one factor ----------------------------------------------------------
+  // G: 0..3 for g1..g4.  MODE: FAC_TILDE applies (I + tK), FAC_TRUE
+  // c(I + tK) = F_g, FAC_INV c(I - tK) = F_g^{-1} (c^2 - s^2 = 1).
+  __device__ static __forceinline__ bool xcross(int G, int r) { return G == 0 ? (r & 1) : !(r & 1); }
+
+  template <int MODE>
+  __device__ __forceinline__ void pair_update(Cx<R>& vi, Cx<R>& vj, Cx<R> a, R c) const {
+    const Cx<R> oi = vi, oj = vj;
+    if (MODE == FAC_INV) a = cneg(a);
+    vi = cfma(a, oj, oi);
+    vj = cjfma(a, oi, oj);
+    if (MODE != FAC_TILDE) {
+      vi = c * vi;
+      vj = c * vj;
+    }
+  }
+
+  template <int G, int MODE>
+  __device__ __forceinline__ void factor(Cx<R> (&v)[BY][2]) {
+    const R c = (G == 0) ? c1 : ch;
+    Cx<R>* buf = xb[cur];
+    if (G == 0 || G == 2) {
+      Cx<R>* xl = buf;
+      Cx<R>* xr = buf + L * nbx;
+      if (on) {
+#pragma unroll
+        for (int r = 0; r < BY; ++r)
+          if (xcross(G, r)) {
+            xl[(y0 + r) * nbx + bx] = v[r][0];
+            xr[(y0 + r) * nbx + bx] = v[r][1];
+          }
+      }
+      __syncthreads();
+      if (on) {
+#pragma unroll
+        for (int r = 0; r < BY; ++r) {
+          if (!xcross(G, r)) {
+            pair_update<MODE>(v[r][0], v[r][1], TPX(r, 0), c);
+          } else {
+            const Cx<R> right = xl[(y0 + r) * nbx + bxr];
+            const Cx<R> left = xr[(y0 + r) * nbx + bxl];
+            Cx<R> ao = TPX(r, 1), al = TPL(r);
+            if (MODE == FAC_INV) {
+              ao = cneg(ao);
+              al = cneg(al);
+            }
+            v[r][1] = cfma(ao, right, v[r][1]);
+            v[r][0] = cjfma(al, left, v[r][0]);
+            if (MODE != FAC_TILDE) {
+              v[r][1] = c * v[r][1];
+              v[r][0] = c * v[r][0];
+            }
+          }
+        }
+      }
+    } else {
+      constexpr int CL = (G == 1) ? 0 : 1;  // column with only local pairs
+      constexpr int CC = 1 - CL;            // column with cross pairs at its ends
+      Cx<R>* yt = buf;
+      Cx<R>* yb = buf + nby * L;
+      if (on) {
+        yt[by * L + x0 + CC] = v[0][CC];
+        yb[by * L + x0 + CC] = v[BY - 1][CC];
+      }
+      __syncthreads();
+      if (on) {
+#pragma unroll
+        for (int r = 0; r < BY; r += 2) pair_update<MODE>(v[r][CL], v[r + 1][CL], TPY(r, CL), c);
+#pragma unroll
+        for (int r = 1; r + 1 < BY; r += 2) pair_update<MODE>(v[r][CC], v[r + 1][CC], TPY(r, CC), c);
+        const Cx<R> below = yt[byd * L + x0 + CC];
+        const Cx<R> above = yb[byu * L + x0 + CC];
+        Cx<R> ab = TPY(BY - 1, CC), at = TPT(CC);
+        if (MODE == FAC_INV) {
+          ab = cneg(ab);
+          at = cneg(at);
+        }
+        Cx<R> nb = cfma(ab, below, v[BY - 1][CC]);
+        Cx<R> nt = cjfma(at, above, v[0][CC]);
+        if (MODE != FAC_TILDE) {
+          nb = c * nb;
+          nt = c * nt;
+        }
+        v[BY - 1][CC] = nb;
+        v[0][CC] = nt;
+      }
+    }
+    cur ^= 1;
+  }
+
+  // B = F4 F3 F2 F1 F2 F3 F4 without the scalar Cb (FAC_TILDE) or exact
+  template <int MODE>
+  __device__ __forceinline__ void applyB(Cx<R> (&v)[BY][2]) {
+    factor<3, MODE>(v);
+    factor<2, MODE>(v);
+    factor<1, MODE>(v);
+    factor<0, MODE>(v);
+    factor<1, MODE>(v);
+    factor<2, MODE>(v);
+    factor<3, MODE>(v);
+  }
+};
+
+// y = a - s * b  (s real)
+template <typename R, int BY>
+__device__ __forceinline__ void axpy_blk(Cx<R> (&y)[BY][2], const Cx<R> (&a)[BY][2], R s,
+                                         const Cx<R> (&b)[BY][2]) {
+#pragma unroll
+  for (int r = 0; r < BY; ++r)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      y[r][c].re = fma(-s, b[r][c].re, a[r][c].re);
+      y[r][c].im = fma(-s, b[r][c].im, a[r][c].im);
+    }
+}
+
+template <typename R, int BY>
+__device__ __forceinline__ void copy_blk(Cx<R> (&y)[BY][2], const Cx<R> (&a)[BY][2]) {
+#pragma unroll
+  for (int r = 0; r < BY; ++r)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) y[r][c] = a[r][c];
+}
+
+// sigma_t: +1 for t < Nt-1 and -1 for the antiperiodic wrap t = Nt-1
+template <typename R>
+__device__ __forceinline__ R sigma_of(int t, int Nt) { return t == Nt - 1 ? R(-1) : R(1); }
+
+}  // namespace qedf

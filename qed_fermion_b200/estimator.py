@@ -1,0 +1,55 @@
+"""Stochastic-estimator solves: G_eta = (M^dag M)^{-1} M^dag eta for Nrv noise
+vectors sharing one gauge field, as one multi-right-hand-side batched PCG.
+
+Mirrors ``StochaticEstimator.random_vec_bin`` / ``set_eta_G_eta`` /
+``set_eta_G_eta_inner`` (``qed_fermion/stochastic_estimator.py:210-224,
+409-433``).  The reference repeats the boson Nrv times and solves with
+``bs = Nrv``; here the Nrv right-hand sides reference one angle array.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+from . import ops
+from .hmc import ref_to_kernel
+from .solver import PcgSolver, System
+
+
+class StochaticEstimator:
+    def __init__(self, Lx, Ltau, Nrv=20, dtau=0.1, precision="mixed", cg_rtol=1e-10, max_iter=20000,
+                 use_precon=True, device=None, seed=None, noise="z2z2"):
+        self.Lx, self.Ly, self.Ltau, self.Nrv, self.dtau = Lx, Lx, Ltau, Nrv, dtau
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        self.noise = noise
+        self.generator = torch.Generator(device=self.device)
+        if seed is not None:
+            self.generator.manual_seed(seed)
+        mode = precision
+        self.solver = PcgSolver([System(Lx, Ltau, Nrv, True)], mode=mode, rtol=cg_rtol, max_iter=max_iter,
+                                dtau=dtau, use_precon=use_precon and Ltau >= 26, device=self.device)
+        self.eta = None
+        self.G_eta = None
+
+    def random_vec_bin(self):
+        """Nrv vectors with entries (+-1 +- i)/sqrt(2) (reference :210-224); with
+        ``noise="z2"`` real +-1 entries instead."""
+        n = self.Lx * self.Ly * self.Ltau
+        re = torch.randint(0, 2, (self.Nrv, n), device=self.device, generator=self.generator) * 2 - 1
+        if self.noise == "z2":
+            return re.to(torch.complex128)
+        im = torch.randint(0, 2, (self.Nrv, n), device=self.device, generator=self.generator) * 2 - 1
+        return (re + 1j * im).to(torch.complex128) / math.sqrt(2.0)
+
+    def set_eta_G_eta(self, boson, eta):
+        """boson: ``[1, 2, Lx, Ly, Ltau]``; eta: ``[Nrv, N]``.  Sets ``self.G_eta``."""
+        self.eta = eta
+        phi = ref_to_kernel(boson)[0]
+        vdt = self.solver.vec_dtype
+        adt = torch.float64 if vdt == torch.complex128 else torch.float32
+        psi = ops.apply_operator("mh", phi.to(adt), eta.to(vdt), self.Lx, self.dtau, rhs_per_boson=self.Nrv)
+        res = self.solver.solve(phi.to(self.solver.angle_dtype), psi)
+        self.G_eta = res.x.view(self.Nrv, -1)
+        self.iters, self.relres, self.status = res.iters, res.relres, res.status
+        return self.G_eta

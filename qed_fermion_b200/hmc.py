@@ -1,0 +1,253 @@
+"""Hybrid Monte Carlo for the fermion-coupled U(1) gauge field on the B200 kernels.
+
+``HmcSampler`` keeps the reference's call signatures
+(``qed_fermion/hmc_sampler_batch.py``): ``draw_momentum`` (:1247),
+``draw_psudo_fermion`` (:1279), ``preconditioned_cg_fast_test`` (:751),
+``Ot_inv_psi_fast`` (:2112), ``force_f_fast`` (:2150), ``leapfrog_cmp``
+(:2332), ``leapfrog_proposer5`` (:2366), ``metropolis_update`` (:2886) and the
+boson action/force methods (:1338-1459).  Bosons, momenta and forces use the
+reference layout ``[bs, 2, Lx, Ly, Ltau]`` at this interface; internally the
+trajectory runs in the kernels' layout ``[bs, Ltau, Ly, Lx, 2]``.
+
+Precision ("precision" argument):
+  "fp64"  plain double path: float64 angles/momenta, complex128 vectors,
+          double PCG and force;
+  "mixed" float32 angles and momenta (as the reference stores them), PCG in
+          float with double reliable updates, float force, and the
+          Hamiltonian, Delta H and the Metropolis test in double;
+  "fp32"  everything in single precision (the reference's own GPU choice).
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+from . import ops
+from .solver import PcgSolver, System
+
+PRECISIONS = ("fp64", "mixed", "fp32")
+
+
+def ref_to_kernel(boson: torch.Tensor) -> torch.Tensor:
+    """``[bs, 2, Lx, Ly, Ltau] -> [bs, Ltau*Ly*Lx*2]`` (``permute([0, 4, 3, 2, 1])``)."""
+    return boson.permute(0, 4, 3, 2, 1).reshape(boson.shape[0], -1).contiguous()
+
+
+def kernel_to_ref(phi: torch.Tensor, Lx: int, Ltau: int) -> torch.Tensor:
+    bs = phi.shape[0]
+    return phi.view(bs, Ltau, Lx, Lx, 2).permute(0, 4, 3, 2, 1).contiguous()
+
+
+class HmcSampler:
+    def __init__(self, Lx=6, Ltau=10, J=1.0, K=1.0, dtau=0.1, bs=1, delta_t=0.06, N_leapfrog=5, m=1.0,
+                 compact=False, precision="mixed", cg_rtol=1e-10, max_iter=20000, use_precon=True,
+                 ru_interval=50, ru_delta=0.1, device=None, seed=None):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {PRECISIONS}")
+        if Lx % 2:
+            raise ValueError("Lx must be even")
+        self.Lx = self.Ly = Lx
+        self.Ltau = Ltau
+        self.Vs = Lx * Lx
+        self.bs = bs
+        self.dtau = dtau
+        self.Nf = 2
+        # couplings as HmcSampler.__init__ scales them (hmc_sampler_batch.py:166-175)
+        self.J = J / dtau * self.Nf / 4
+        self.K = K * dtau * self.Nf / 2
+        self.t = 1
+        self.m = m
+        self.compact = compact
+        self.N_leapfrog = N_leapfrog
+        self.precision = precision
+        self.cg_rtol = cg_rtol
+        self.max_iter = max_iter
+        self.use_precon = use_precon and Ltau >= 26
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        self.dtype = torch.float64 if precision == "fp64" else torch.float32
+        self.cdtype = torch.complex128 if precision in ("fp64", "mixed") else torch.complex64
+        self.delta_t_tensor = torch.full((bs,), float(delta_t), device=self.device, dtype=torch.float64)
+        self.generator = torch.Generator(device=self.device)
+        if seed is not None:
+            self.generator.manual_seed(seed)
+        solver_mode = {"fp64": "fp64", "mixed": "mixed", "fp32": "fp32"}[precision]
+        self.solver = PcgSolver([System(Lx, Ltau, bs, False)], mode=solver_mode, rtol=cg_rtol, max_iter=max_iter,
+                                dtau=dtau, use_precon=self.use_precon, ru_interval=ru_interval,
+                                ru_delta=ru_delta, device=self.device)
+        self.boson = None
+        self.last_cg_iters = None
+
+    # ---- couplings ---------------------------------------------------------
+    @property
+    def tau_coeff(self):
+        return 1.0 / self.J / self.dtau ** 2
+
+    # ---- initial fields (reference :1026-1043) --------------------------------
+    def initialize_boson_pi_flux_randn_matfree(self):
+        x = torch.arange(self.Lx, device=self.device).view(-1, 1)
+        y = torch.arange(self.Ly, device=self.device).view(1, -1)
+        sign = (1 - 2 * ((x + y) % 2)).to(self.dtype)
+        stag = torch.zeros(1, 2, self.Lx, self.Ly, self.Ltau, device=self.device, dtype=self.dtype)
+        stag[0, 0] = (sign * math.pi / 4).unsqueeze(-1)
+        stag[0, 1] = (-sign * math.pi / 4).unsqueeze(-1)
+        if self.bs > 1:
+            noise = torch.randn(self.bs - 1, 2, self.Lx, self.Ly, 1, device=self.device, dtype=self.dtype,
+                                generator=self.generator)
+            lev = torch.linspace(0.02, 0.08, self.bs - 1, device=self.device, dtype=self.dtype).view(-1, 1, 1, 1, 1)
+            self.boson = torch.cat([stag.repeat(self.bs - 1, 1, 1, 1, 1) + noise * lev, stag], dim=0)
+        else:
+            self.boson = stag
+        return self.boson
+
+    # ---- random draws (reference :1247-1252, :1279-1287) ----------------------
+    def draw_momentum(self):
+        return torch.randn(self.bs, 2, self.Lx, self.Ly, self.Ltau, device=self.device, dtype=self.dtype,
+                           generator=self.generator) * math.sqrt(self.m)
+
+    def draw_psudo_fermion(self):
+        # the reference's active line: complex randn (E|z|^2 = 1) divided by sqrt(2)
+        return torch.randn(self.bs, self.Vs * self.Ltau, device=self.device, dtype=self.cdtype,
+                           generator=self.generator) / math.sqrt(2)
+
+    # ---- boson action and forces (reference layout) ---------------------------
+    def action_boson_tau(self, x):
+        phi = ref_to_kernel(x)
+        return ops.boson_action(phi, self.Lx, 0.0, self.tau_coeff, self.compact)
+
+    def action_boson_plaq_matfree(self, x):
+        phi = ref_to_kernel(x)
+        return ops.boson_action(phi, self.Lx, self.K, 0.0, self.compact)
+
+    def force_b_plaq_matfree(self, x):
+        phi = ref_to_kernel(x)
+        return kernel_to_ref(ops.boson_force(phi, self.Lx, self.K, 0.0), self.Lx, self.Ltau)
+
+    def force_b_tau_noncmp(self, x):
+        phi = ref_to_kernel(x)
+        return kernel_to_ref(ops.boson_force(phi, self.Lx, 0.0, self.tau_coeff, False), self.Lx, self.Ltau)
+
+    def force_b_tau_cmp(self, x):
+        phi = ref_to_kernel(x)
+        return kernel_to_ref(ops.boson_force(phi, self.Lx, 0.0, self.tau_coeff, True), self.Lx, self.Ltau)
+
+    # ---- solver ---------------------------------------------------------------
+    def _angles_for_solver(self, phi_k):
+        return phi_k.to(self.solver.angle_dtype)
+
+    def Ot_inv_psi_fast(self, psi, boson_k, MhM=None):
+        """xi = (M^dag M)^{-1} psi with the persistent batched PCG.
+        ``boson_k``: kernel-layout angles ``[bs, ...]``; returns (xi, iters, relres)."""
+        res = self.solver.solve(self._angles_for_solver(boson_k), psi.to(self.solver.vec_dtype))
+        self.last_cg_iters = res.iters
+        self.last_status = res.status
+        return res.x.view(self.bs, -1), res.iters, res.relres
+
+    def preconditioned_cg_fast_test(self, boson, b, MhM_inv=None, matL=None, b_idx=None, axs=None,
+                                    cg_dtype=None, MhM=None, precon_tau=None):
+        """The reference's batched masked PCG loop (``hmc_sampler_batch.py:751-846``),
+        one torch/_C launch sequence per iteration, on this library's kernels.
+        ``boson``: ``[bs, Ltau, Vs*2]`` angles; ``b``: ``[bs, N]``.  Runs until
+        every system converged or ``max_iter``; returns (x, iterations, error)."""
+        bs = b.shape[0]
+        boson = boson.reshape(bs, -1)
+        dt = self.dtau
+        norm_b = torch.linalg.vector_norm(b, dim=1)
+        active = torch.ones((bs, 1), device=b.device, dtype=b.dtype)
+        x = torch.zeros_like(b)
+
+        def P(r):
+            return ops.precon_apply(r, precon_tau, self.Lx) if precon_tau is not None else r.clone()
+
+        r = b - ops.apply_operator("mhm", boson, x, self.Lx, dt)
+        z = P(r)
+        p = z
+        rz_old = torch.einsum("bj,bj->b", r.conj(), z).real
+        iterations = torch.zeros(bs, dtype=torch.int64, device=b.device)
+        error = torch.ones(bs, dtype=norm_b.dtype, device=b.device)
+        for _ in range(self.max_iter):
+            Op = ops.apply_operator("mhm", boson, p, self.Lx, dt)
+            alpha = (rz_old / torch.einsum("bj,bj->b", p.conj(), Op).real).unsqueeze(-1)
+            x = x + alpha * p * active
+            r = r - alpha * Op * active
+            error = torch.linalg.vector_norm(r, dim=1) / norm_b
+            active = torch.where(error.view(-1, 1) > self.cg_rtol, active, torch.zeros_like(active))
+            if bool((active == 0).all()):
+                break
+            iterations += (active == 1).view(-1).long()
+            z = P(r)
+            rz_new = torch.einsum("bj,bj->b", r.conj(), z).real
+            beta = rz_new / rz_old
+            p = z + beta.unsqueeze(-1) * p * active
+            rz_old = rz_new
+        return x, iterations, error
+
+    # ---- fermion force (reference :2150-2227) ---------------------------------
+    def force_f_fast(self, psi, boson, MhM=None):
+        """Returns (Ft [bs, 2, Lx, Ly, Ltau], xi [bs, N], cg_iters, r_err)."""
+        phi_k = ref_to_kernel(boson)
+        xi, it, err = self.Ot_inv_psi_fast(psi, phi_k)
+        F = self._force_from_xi(phi_k, xi)
+        return kernel_to_ref(F, self.Lx, self.Ltau), xi, it, err
+
+    def _force_from_xi(self, phi_k, xi):
+        if self.precision == "fp64":
+            return ops.fermion_force(phi_k, xi, self.Lx, self.dtau)
+        return ops.fermion_force(phi_k.to(torch.float32), xi.to(torch.complex64), self.Lx, self.dtau).to(self.dtype)
+
+    # ---- trajectory -------------------------------------------------------------
+    def _Sb_kin(self, phi_k, p_k):
+        # S_tau + S_plaq + sum p^2 / 2m in double
+        return ops.boson_action(phi_k, self.Lx, self.K, self.tau_coeff, self.compact, momenta=p_k, mass=self.m)
+
+    def leapfrog_proposer5(self, boson, tau_mask=None, p0=None, R=None):
+        """One trajectory from ``boson`` (reference layout); ``p0`` / ``R`` may
+        be given (reference layout / ``[bs, N]``) instead of drawn.
+        Returns (x, H0, H_fin, cg_iters_mean, r_err_mean) like the reference."""
+        Lx, Ltau = self.Lx, self.Ltau
+        if p0 is None:
+            p0 = self.draw_momentum()
+        if R is None:
+            R = self.draw_psudo_fermion()
+        x = ref_to_kernel(boson.to(self.dtype))
+        p = ref_to_kernel(p0.to(self.dtype))
+        mask = None
+        if tau_mask is not None:
+            mask = tau_mask.reshape(-1).to(torch.float32).contiguous()
+        dt = self.delta_t_tensor
+        # psi = M(x0)^dag R, in the solver's vector precision
+        vdt = self.solver.vec_dtype
+        adt = torch.float64 if vdt == torch.complex128 else torch.float32
+        psi = ops.apply_operator("mh", x.to(adt), R.to(vdt).reshape(self.bs, -1), Lx, self.dtau)
+        xi, it, err = self.Ot_inv_psi_fast(psi, x)
+        iters, errs = [it.to(torch.float64)], [err]
+        Ff = self._force_from_xi(x, xi)
+        Sf0 = ops.cdot(psi, xi)
+        H0 = self._Sb_kin(x, p) + Sf0
+        Fb = ops.boson_force(x, Lx, self.K, self.tau_coeff, self.compact)
+        M = 5
+        for _ in range(self.N_leapfrog):
+            ops.kick_drift(p, Ff, None, dt, mask, 0.5, 0.0, Lx)
+            for _ in range(M):
+                ops.kick_drift(p, Fb, x, dt, mask, 0.5 / M, 1.0 / M / self.m, Lx)
+                ops.boson_force(x, Lx, self.K, self.tau_coeff, self.compact, out=Fb)
+                ops.kick_drift(p, Fb, None, dt, mask, 0.5 / M, 0.0, Lx)
+            xi, it, err = self.Ot_inv_psi_fast(psi, x)
+            iters.append(it.to(torch.float64))
+            errs.append(err)
+            Ff = self._force_from_xi(x, xi)
+            ops.kick_drift(p, Ff, None, dt, mask, 0.5, 0.0, Lx)
+        Sf = ops.cdot(psi, xi)
+        H_fin = self._Sb_kin(x, p) + Sf
+        self._last_p = p
+        return (kernel_to_ref(x, Lx, Ltau), H0, H_fin, torch.stack(iters).mean(dim=0),
+                torch.stack(errs).mean(dim=0))
+
+    def metropolis_update(self, tau_mask=None):
+        """One Metropolis step on ``self.boson`` (reference :2886-2930); the
+        accept test ``u < exp(H_old - H_new)`` is evaluated in double."""
+        boson_new, H_old, H_new, it, err = self.leapfrog_proposer5(self.boson, tau_mask)
+        u = torch.rand(self.bs, device=self.device, dtype=torch.float64, generator=self.generator)
+        accp = u < torch.exp(H_old - H_new)
+        self.boson = torch.where(accp.view(-1, 1, 1, 1, 1), boson_new.to(self.boson.dtype), self.boson)
+        return self.boson, accp, it, err, H_old, H_new

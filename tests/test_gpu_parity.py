@@ -1,0 +1,359 @@
+"""GPU parity of the sm_100a kernels against the CPU oracle (C ABI via ctypes).
+
+Tolerances (relative to the largest magnitude of the reference result):
+operators 1e-13 in complex128 and 1e-6 in complex64 (the stated bar for the
+matvec), force 1e-12 / 2e-5, solver solutions at the solver tolerance.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import qedf_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEV = torch.device("cuda:0") if torch.cuda.is_available() else None
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from qed_fermion_b200 import build
+    build.build()
+    torch.cuda.set_device(DEV)
+
+
+def relerr(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def rand_case(L, Nt, bs, seed, kind="uniform"):
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        boson = rng.uniform(-np.pi, np.pi, size=(bs, 2, L, L, Nt))
+    else:
+        x = np.arange(L)[:, None]
+        y = np.arange(L)[None, :]
+        sg = 1 - 2 * ((x + y) % 2)
+        boson = np.zeros((bs, 2, L, L, Nt))
+        boson[:, 0] = (sg * np.pi / 4)[None, :, :, None]
+        boson[:, 1] = (-sg * np.pi / 4)[None, :, :, None]
+        boson += 0.1 * rng.standard_normal(boson.shape)
+    v = (rng.standard_normal((bs, Nt * L * L)) + 1j * rng.standard_normal((bs, Nt * L * L))) / np.sqrt(2)
+    return boson, v
+
+
+OPS = {"m": O.m_vec, "mh": O.mh_vec, "mhm": O.mhm_vec}
+
+
+@pytest.mark.parametrize("L,Nt,bs,by,slab", [
+    (2, 6, 1, 0, 0), (4, 10, 2, 0, 0), (4, 10, 1, 4, 3), (6, 20, 3, 0, 0), (6, 20, 1, 6, 7),
+    (12, 24, 2, 0, 5), (12, 24, 1, 4, 1), (30, 12, 1, 0, 0), (36, 8, 1, 6, 0), (48, 8, 1, 0, 0),
+    (48, 8, 1, 4, 3), (66, 6, 1, 0, 0)])
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+@pytest.mark.parametrize("op", ["m", "mh", "mhm"])
+def test_operator_matches_oracle(op, prec, L, Nt, bs, by, slab):
+    from qed_fermion_b200 import _lib, ops
+    if prec == "c128" and L == 66:
+        # the double-precision slice engine of a 66 x 66 slice needs more shared
+        # memory than a thread block has: the library reports a size error
+        x = torch.zeros((1, L * L * Nt), dtype=torch.complex128, device=DEV)
+        with pytest.raises(_lib.QedfError) as ei:
+            ops.apply_operator(op, torch.zeros((1, 2 * L * L * Nt), dtype=torch.float64, device=DEV), x, L, 0.1)
+        assert ei.value.status == _lib.QEDF_ERR_SIZE
+        return
+    boson, v = rand_case(L, Nt, bs, seed=L * 1000 + Nt)
+    phi = O.ref_to_kernel_layout(boson)
+    want = OPS[op](phi, v.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    cdt, rdt = (torch.complex64, torch.float32) if prec == "c64" else (torch.complex128, torch.float64)
+    got = ops.apply_operator(op, torch.tensor(phi.reshape(bs, -1), dtype=rdt, device=DEV),
+                             torch.tensor(v, dtype=cdt, device=DEV), L, 0.1, by=by, slab=slab)
+    tol = 1e-6 if prec == "c64" else 1e-13
+    assert relerr(got.cpu().numpy(), want) < tol
+
+
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+def test_operator_shared_boson_rows(prec):
+    """Several vectors referencing one angle array (the estimator's layout)."""
+    from qed_fermion_b200 import ops
+    L, Nt, nrv = 6, 12, 4
+    boson, v = rand_case(L, Nt, nrv, seed=5)
+    boson = np.repeat(boson[:1], nrv, axis=0)
+    phi = O.ref_to_kernel_layout(boson)
+    want = O.mhm_vec(phi, v.reshape(nrv, Nt, L * L), L, 0.1).reshape(nrv, -1)
+    cdt, rdt = (torch.complex64, torch.float32) if prec == "c64" else (torch.complex128, torch.float64)
+    got = ops.apply_operator("mhm", torch.tensor(phi[:1].reshape(1, -1), dtype=rdt, device=DEV),
+                             torch.tensor(v, dtype=cdt, device=DEV), L, 0.1, rhs_per_boson=nrv)
+    assert relerr(got.cpu().numpy(), want) < (1e-6 if prec == "c64" else 1e-13)
+
+
+def test_golden_operator_fixture():
+    """The reference's own M, M^dag, M^dag M on its sparse matrices (complex128)."""
+    from qed_fermion_b200 import ops
+    G = dict(np.load(os.path.join(HERE, "golden", "golden_ref.npz")))
+    for tag in ("L4_T10", "L6_T20", "L4_T30"):
+        L = int(tag.split("_")[0][1:])
+        phi = torch.tensor(O.ref_to_kernel_layout(G[f"op_{tag}_boson"]).reshape(1, -1), device=DEV)
+        x = torch.tensor(G[f"op_{tag}_x"].reshape(1, -1), device=DEV)
+        for op, key in (("m", "Mx"), ("mh", "MHx"), ("mhm", "MHMx")):
+            got = ops.apply_operator(op, phi, x, L, 0.1).cpu().numpy().reshape(-1)
+            assert relerr(got, G[f"op_{tag}_{key}"]) < 1e-13, (tag, op)
+
+
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+@pytest.mark.parametrize("interm", [False, True])
+def test_b_vec_per_tau(prec, interm):
+    from qed_fermion_b200 import _C
+    G = dict(np.load(os.path.join(HERE, "golden", "golden_ref.npz")))
+    for tag in ("L4_T10", "L6_T20"):
+        L = int(tag.split("_")[0][1:])
+        tau = int(G[f"bvec_{tag}_tau"])
+        phi = O.ref_to_kernel_layout(G[f"op_{tag}_boson"])[0, tau]
+        v = G[f"bvec_{tag}_v"]
+        rows = G[f"bvec_{tag}_rows"]
+        cdt, rdt = (torch.complex64, torch.float32) if prec == "c64" else (torch.complex128, torch.float64)
+        vt = torch.tensor(v, dtype=cdt, device=DEV)
+        got = _C.b_vec_per_tau(torch.tensor(phi, dtype=rdt, device=DEV), vt, L, 0.1, interm, 4, 8)
+        want = rows[:6] if interm else rows[6]
+        assert relerr(got.cpu().numpy(), want) < (1e-6 if prec == "c64" else 1e-13)
+        # a lazily conjugated argument is read through its raw storage
+        got_c = _C.b_vec_per_tau(torch.tensor(phi, dtype=rdt, device=DEV), vt.conj(), L, 0.1, interm, 4, 8)
+        assert torch.equal(got_c, got)
+
+
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+def test_precon_vec_dropin(prec):
+    """_C.precon_vec with the reference's N x N CSR (built as P_tau (x) I)."""
+    from qed_fermion_b200 import _C
+    L, Nt, bs = 4, 30, 3
+    P_tau = O.precon_tau_matrix(Nt)
+    cdt = torch.complex64 if prec == "c64" else torch.complex128
+    csr = torch.tensor(np.kron(P_tau, np.eye(L * L)), dtype=cdt).to_sparse_csr().to(DEV)
+    rng = np.random.default_rng(1)
+    r = rng.standard_normal((bs, Nt * L * L)) + 1j * rng.standard_normal((bs, Nt * L * L))
+    want = O.precon_vec(r.reshape(bs, Nt, L * L), P_tau).reshape(bs, -1)
+    got = _C.precon_vec(torch.tensor(r, dtype=cdt, device=DEV), csr, L)
+    assert relerr(got.cpu().numpy(), want) < (1e-6 if prec == "c64" else 1e-14)
+
+
+@pytest.mark.parametrize("L,Nt,bs", [(4, 10, 1), (6, 20, 2), (12, 12, 1), (48, 4, 1), (66, 3, 1)])
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+def test_force_matches_oracle(prec, L, Nt, bs):
+    from qed_fermion_b200 import ops
+    if prec == "c128" and L == 66:
+        pytest.skip("double-precision force at L=66 exceeds the shared-memory budget (mixed path uses float)")
+    boson, xi = rand_case(L, Nt, bs, seed=11 + L)
+    phi = O.ref_to_kernel_layout(boson)
+    want = O.force_f_from_xi(phi, xi.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    cdt, rdt = (torch.complex64, torch.float32) if prec == "c64" else (torch.complex128, torch.float64)
+    got = ops.fermion_force(torch.tensor(phi.reshape(bs, -1), dtype=rdt, device=DEV),
+                            torch.tensor(xi, dtype=cdt, device=DEV), L, 0.1)
+    assert relerr(got.cpu().numpy(), want) < (2e-5 if prec == "c64" else 1e-12)
+
+
+def test_force_golden_fixture():
+    from qed_fermion_b200 import ops
+    G = dict(np.load(os.path.join(HERE, "golden", "golden_ref.npz")))
+    for tag in ("L4_T10", "L6_T20"):
+        L = int(tag.split("_")[0][1:])
+        Nt = int(tag.split("_")[1][1:])
+        phi = O.ref_to_kernel_layout(G[f"force_{tag}_boson"])
+        got = ops.fermion_force(torch.tensor(phi.reshape(1, -1), device=DEV),
+                                torch.tensor(G[f"force_{tag}_xi"].reshape(1, -1), device=DEV), L, 0.1)
+        F = O.kernel_to_ref_layout(got.cpu().numpy().reshape(1, Nt, -1), L)
+        assert relerr(F.reshape(-1), G[f"force_{tag}_F"].reshape(-1)) < 1e-11
+
+
+def test_autograd_force_central_differences():
+    """dS_f/dphi from the adjoint kernel vs central differences of S_f (h = 1e-5)."""
+    from qed_fermion_b200.force import fermion_action
+    from qed_fermion_b200.solver import PcgSolver, System
+    L, Nt = 4, 10
+    boson, psi = rand_case(L, Nt, 1, seed=3)
+    phi = torch.tensor(O.ref_to_kernel_layout(boson).reshape(1, -1), device=DEV, requires_grad=True)
+    psi_t = torch.tensor(psi, device=DEV)
+    solver = PcgSolver([System(L, Nt, 1)], mode="fp64", rtol=1e-14, max_iter=50000, device=DEV)
+    S = fermion_action(phi, psi_t, solver, L, 0.1)
+    (g,) = torch.autograd.grad(S.sum(), phi)
+    rng = np.random.default_rng(0)
+    h = 1e-5
+    for k in rng.choice(phi.numel(), 16, replace=False):
+        with torch.no_grad():
+            pp = phi.detach().clone()
+            pp[0, k] += h
+            pm = phi.detach().clone()
+            pm[0, k] -= h
+            fd = (fermion_action(pp, psi_t, solver, L, 0.1) - fermion_action(pm, psi_t, solver, L, 0.1)) / (2 * h)
+        assert abs(float(fd) - float(g[0, k])) < 1e-6 * max(1.0, abs(float(g[0, k]))), k
+
+
+def _solve_oracle(phi_k, b, L, Nt, P_tau, rtol):
+    bs = b.shape[0]
+    A = lambda v: O.mhm_vec(phi_k, v.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    Pf = None if P_tau is None else (lambda v: O.precon_vec(v.reshape(bs, Nt, L * L), P_tau).reshape(bs, -1))
+    return O.pcg_batched_masked(A, b, Pf, rtol, 20000, reference_alias=False)
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed", "fp32"])
+@pytest.mark.parametrize("L,Nt,bs,kind", [(4, 10, 2, "uniform"), (4, 30, 2, "piflux"), (6, 40, 1, "piflux")])
+def test_pcg_solves(mode, L, Nt, bs, kind):
+    from qed_fermion_b200.solver import PcgSolver, System
+    boson, b = rand_case(L, Nt, bs, seed=21 + Nt, kind=kind)
+    phi = O.ref_to_kernel_layout(boson)
+    rtol = 1e-5 if mode == "fp32" else 1e-10
+    solver = PcgSolver([System(L, Nt, bs)], mode=mode, rtol=rtol, max_iter=20000, device=DEV)
+    rdt = solver.angle_dtype
+    res = solver.solve(torch.tensor(phi.reshape(bs, -1), dtype=rdt, device=DEV),
+                       torch.tensor(b, dtype=solver.vec_dtype, device=DEV))
+    assert res.status.cpu().tolist() == [0] * bs
+    x = res.x.cpu().numpy().reshape(bs, -1)
+    # the true residual of the returned x, with the oracle's operator on the same angles
+    phi_used = phi.astype(np.float32).astype(np.float64) if rdt == torch.float32 else phi
+    r = b - O.mhm_vec(phi_used, x.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    true_rel = np.linalg.norm(r, axis=1) / np.linalg.norm(b, axis=1)
+    assert np.all(true_rel < (5 * rtol if mode == "fp32" else 2 * rtol)), true_rel
+    xo, _, _ = _solve_oracle(phi_used, b, L, Nt, O.precon_tau_matrix(Nt) if Nt >= 26 else None, 1e-13)
+    assert relerr(x, xo) < (1e-3 if mode == "fp32" else 1e-7)
+
+
+def test_pcg_batch_of_uneven_lattices():
+    """Several lattices of different L and Ltau in one launch, each with its own mask."""
+    from qed_fermion_b200.solver import PcgSolver, System
+    systems = [System(4, 30, 2), System(6, 40, 1), System(4, 12, 1), System(8, 26, 3, True)]
+    phis, bs_, refs = [], [], []
+    for k, s in enumerate(systems):
+        nb = 1 if s.shared_boson else s.nrhs
+        boson, b = rand_case(s.Lx, s.Ltau, s.nrhs, seed=100 + k, kind="piflux")
+        phi = O.ref_to_kernel_layout(boson[:nb])
+        phis.append(phi.reshape(-1))
+        bs_.append(b.reshape(-1))
+        refs.append((s, phi, b))
+    solver = PcgSolver(systems, mode="mixed", rtol=1e-10, max_iter=20000, device=DEV)
+    res = solver.solve(torch.tensor(np.concatenate(phis), dtype=torch.float32, device=DEV),
+                       torch.tensor(np.concatenate(bs_), device=DEV))
+    assert res.status.cpu().tolist() == [0] * solver.nrhs
+    x = res.x.cpu().numpy()
+    off = 0
+    for s, phi, b in refs:
+        n = s.n * s.nrhs
+        xs = x[off:off + n].reshape(s.nrhs, s.Ltau, s.Lx * s.Lx)
+        off += n
+        ph = phi.astype(np.float32).astype(np.float64)
+        if s.shared_boson:
+            ph = np.repeat(ph, s.nrhs, axis=0)
+        r = b - O.mhm_vec(ph, xs, s.Lx, 0.1).reshape(s.nrhs, -1)
+        assert np.all(np.linalg.norm(r, axis=1) / np.linalg.norm(b, axis=1) < 2e-10)
+    its = res.iters.cpu().tolist()
+    assert len(set(its)) > 1  # the masks stopped the systems at different iterations
+
+
+def test_pcg_status_codes():
+    from qed_fermion_b200 import _lib
+    from qed_fermion_b200.solver import PcgSolver, System
+    L, Nt = 4, 30
+    boson, b = rand_case(L, Nt, 2, seed=9)
+    b[1] = 0  # zero right-hand side: exact x = 0, no iteration
+    phi = torch.tensor(O.ref_to_kernel_layout(boson).reshape(2, -1), device=DEV)
+    bt = torch.tensor(b, device=DEV)
+    res = PcgSolver([System(L, Nt, 2)], mode="fp64", rtol=1e-10, max_iter=3, device=DEV).solve(phi, bt)
+    assert res.status.cpu().tolist() == [_lib.QEDF_ERR_MAXITER, 0]
+    assert res.iters.cpu().tolist() == [3, 0]
+    assert float(res.x.view(2, -1)[1].abs().max()) == 0.0
+    # a grid-barrier budget that runs out ends the kernel with a timeout status
+    res = PcgSolver([System(L, Nt, 2)], mode="fp64", rtol=1e-10, max_iter=100, timeout_ms=1e-6,
+                    device=DEV).solve(phi, bt)
+    torch.cuda.synchronize()
+    assert set(res.status.cpu().tolist()) == {_lib.QEDF_ERR_TIMEOUT}
+    # the context stays usable
+    res = PcgSolver([System(L, Nt, 2)], mode="fp64", rtol=1e-10, max_iter=5000, device=DEV).solve(phi, bt)
+    assert res.status.cpu().tolist() == [0, 0]
+
+
+def test_reference_structured_pcg_loop():
+    """HmcSampler.preconditioned_cg_fast_test (the reference's per-iteration
+    loop on this library's _C kernels) against the oracle restatement."""
+    from qed_fermion_b200 import precon
+    from qed_fermion_b200.hmc import HmcSampler
+    L, Nt, bs = 4, 30, 2
+    boson, b = rand_case(L, Nt, bs, seed=4, kind="piflux")
+    hmc = HmcSampler(Lx=L, Ltau=Nt, bs=bs, precision="fp64", cg_rtol=1e-10, max_iter=2000, device=DEV)
+    phi = torch.tensor(O.ref_to_kernel_layout(boson), device=DEV)
+    tau = precon.to_device(precon.builtin_tau_csr(Nt), DEV)
+    x, it, err = hmc.preconditioned_cg_fast_test(phi, torch.tensor(b, device=DEV), precon_tau=tau)
+    P = O.precon_tau_matrix(Nt)
+    A = lambda v: O.mhm_vec(O.ref_to_kernel_layout(boson), v.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    Pf = lambda v: O.precon_vec(v.reshape(bs, Nt, L * L), P).reshape(bs, -1)
+    xo, ito, erro = O.pcg_batched_masked(A, b, Pf, 1e-10, 2000)
+    assert np.all(np.abs(it.cpu().numpy() - ito) <= 1)
+    assert relerr(x.cpu().numpy(), xo) < 1e-8
+
+
+def test_boson_action_and_force():
+    from qed_fermion_b200.hmc import HmcSampler
+    G = dict(np.load(os.path.join(HERE, "golden", "golden_ref.npz")))
+    b = torch.tensor(G["boson_b"], device=DEV)
+    hmc = HmcSampler(Lx=6, Ltau=20, bs=2, precision="fp64", device=DEV)
+    assert relerr(hmc.action_boson_tau(b).cpu(), G["boson_S_tau"]) < 1e-13
+    assert relerr(hmc.action_boson_plaq_matfree(b).cpu(), G["boson_S_plaq"]) < 1e-12
+    assert relerr(hmc.force_b_plaq_matfree(b).cpu(), G["boson_F_plaq"]) < 1e-13
+    assert relerr(hmc.force_b_tau_noncmp(b).cpu(), G["boson_F_tau"]) < 1e-13
+    assert relerr(hmc.force_b_tau_cmp(b).cpu(), G["boson_F_tau_cmp"]) < 1e-13
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_trajectory_matches_reference_fixture(precision):
+    """One trajectory (L=6, Ltau=20, 10 leapfrog steps, rtol 1e-10) from the
+    reference's own leapfrog_proposer5 in complex128, same p0 and R."""
+    from qed_fermion_b200.hmc import HmcSampler
+    T = dict(np.load(os.path.join(HERE, "golden", "golden_traj.npz")))
+    hmc = HmcSampler(Lx=6, Ltau=20, bs=1, precision=precision, cg_rtol=1e-10, max_iter=20000,
+                     delta_t=float(T["traj_delta_t"]), N_leapfrog=int(T["traj_n_leapfrog"]), device=DEV)
+    x, H0, H1, it, err = hmc.leapfrog_proposer5(torch.tensor(T["traj_boson"], device=DEV),
+                                                p0=torch.tensor(T["traj_p0"], device=DEV),
+                                                R=torch.tensor(T["traj_R"], device=DEV))
+    H0r, H1r = T["traj_H0"][0], T["traj_Hfin"][0]
+    dH, dHr = float(H1 - H0), float(H1r - H0r)
+    if precision == "fp64":
+        assert abs(float(H0) - H0r) < 1e-11 * abs(H0r)
+        assert abs(dH - dHr) < 1e-9 * abs(H0r)
+        assert relerr(x.cpu().numpy(), T["traj_x"]) < 1e-9
+    else:
+        # stated bar: Delta H within 1e-6 of |H0| against the FP64 oracle
+        assert abs(dH - dHr) < 1e-6 * abs(H0r), (dH, dHr)
+        assert relerr(x.cpu().numpy(), T["traj_x"]) < 1e-4
+
+
+def test_estimator_matches_ground_truth():
+    from qed_fermion_b200.estimator import StochaticEstimator
+    G = dict(np.load(os.path.join(HERE, "golden", "golden_ref.npz")))
+    eta = G["se_eta"]
+    se = StochaticEstimator(4, 10, Nrv=eta.shape[0], precision="mixed", cg_rtol=1e-11, device=DEV)
+    Gx = se.set_eta_G_eta(torch.tensor(G["se_boson"], device=DEV), torch.tensor(eta, device=DEV))
+    assert relerr(Gx.cpu().numpy(), G["se_G_eta"]) < 1e-6  # float32 angles of a float64 field
+    se64 = StochaticEstimator(4, 10, Nrv=eta.shape[0], precision="fp64", cg_rtol=1e-12, device=DEV)
+    Gx = se64.set_eta_G_eta(torch.tensor(G["se_boson"], device=DEV), torch.tensor(eta, device=DEV))
+    assert relerr(Gx.cpu().numpy(), G["se_G_eta"]) < 1e-9
+
+
+def test_dropin_mhm_mh_signatures():
+    """The reference calls _C.mhm_vec(boson.view(bs, -1), x, Lx, dtau, *BLOCK_SIZE)."""
+    from qed_fermion_b200 import _C
+    L, Nt, bs = 6, 20, 2
+    boson, x = rand_case(L, Nt, bs, seed=8)
+    phi = O.ref_to_kernel_layout(boson).astype(np.float32)
+    pt = torch.tensor(phi, device=DEV).view(bs, Nt, -1)
+    xt = torch.tensor(x, dtype=torch.complex64, device=DEV)
+    got = _C.mhm_vec(pt.view(bs, -1), xt, L, 0.1, 4, 8)
+    want = O.mhm_vec(phi.astype(np.float64), x.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    assert relerr(got.cpu().numpy(), want) < 1e-6
+    got = _C.mh_vec(pt.reshape(bs, -1), xt, L, 0.1, 4, 8)
+    want = O.mh_vec(phi.astype(np.float64), x.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    assert relerr(got.cpu().numpy(), want) < 1e-6
+    with pytest.raises(RuntimeError):
+        _C.mhm_vec(pt.view(bs, -1).double(), xt, L, 0.1, 4, 8)  # dtype mismatch
