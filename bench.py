@@ -53,6 +53,8 @@ def parse_args(argv=None):
     ap.add_argument("--cg-iters-per-solve", type=float, default=None,
                     help="reference arm: PCG iterations per solve used to extrapolate a trajectory")
     ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--quick", action="store_true",
+                    help="timed trajectories only (no e2e, FP64, Delta H, matvec or CPU legs): for profiling")
     return ap.parse_args(argv)
 
 
@@ -327,7 +329,7 @@ def run_native(args):
 
     # --- end to end through the public API with host buffers
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.quick:
         hb = torch.empty((bs, 2, L, L, Lt), dtype=torch.float32, pin_memory=True)
         hb.copy_(hmc.boson.cpu())
         hout = torch.empty_like(hb).pin_memory()
@@ -352,7 +354,7 @@ def run_native(args):
 
     # --- plain FP64 path, same workload
     fp64 = None
-    if rank == 0 and args.fp64_steps > 0:
+    if rank == 0 and args.fp64_steps > 0 and not args.quick:
         h64 = make("fp64")
         h64.boson = hmc.boson.to(torch.float64)
         h64.metropolis_update()
@@ -370,7 +372,7 @@ def run_native(args):
 
     # --- Delta H of one shared trajectory, mixed vs FP64
     dH = None
-    if rank == 0:
+    if rank == 0 and not args.quick:
         h64 = make("fp64")
         gen = torch.Generator(device=dev)
         gen.manual_seed(seed + 7)
@@ -387,7 +389,7 @@ def run_native(args):
 
     # --- M^dag M matvec bandwidth (several right-hand sides, working set > L2)
     mhm = None
-    if rank == 0:
+    if rank == 0 and args.mhm_rhs > 0 and not args.quick:
         nr = args.mhm_rhs
         mhm = {}
         for prec, cdt, rdt, bps in (("c64", torch.complex64, torch.float32, 24), ("c128", torch.complex128,
@@ -414,7 +416,7 @@ def run_native(args):
 
     # --- CPU baseline (oracle restatement) on a bounded sample
     cpu = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and args.cpu_seconds > 0 and not args.quick:
         t_it, t_force, sample = cpu_sample(L, Lt, seed, args.cpu_seconds)
         ips = result.get("cg_iters_per_solve") or 250
         cpu = {"value": cpu_traj_per_hour(t_it, t_force, ips, args.n_leapfrog), "unit": UNIT, "cores": 1,

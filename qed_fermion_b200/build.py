@@ -11,7 +11,7 @@ LIB = os.path.join(HERE, "libqedf.so")
 SOURCES = ["qedf_ops.cu", "qedf_pcg.cu", "qedf_capi.cu"]
 HEADERS = ["qedf_common.cuh", "qedf_slice.cuh", "qedf_internal.h", "qedf_precon_table.h"]
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-         "-Xcompiler", "-fPIC", "-diag-suppress", "20013,20015", "-shared"]
+         "-Xcompiler", "-fPIC", "-diag-suppress", "20013,20015"]
 
 
 def _newest_input():
@@ -25,13 +25,26 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest_input():
         return LIB
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    # one nvcc per translation unit, in parallel, then one link
+    procs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        procs.append((src, subprocess.Popen([nvcc] + FLAGS + ["-c", "-o", obj, src], cwd=CSRC,
+                                            stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    for src, pr in procs:
+        out, err = pr.communicate()
+        if pr.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src} ({pr.returncode}):\n{err[-4000:]}")
+        if verbose:
+            print(err[-2000:])
     tmp = LIB + ".tmp"
-    cmd = [nvcc] + FLAGS + ["-o", tmp] + SOURCES
-    res = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
+    objs = [os.path.join(objdir, s.replace(".cu", ".o")) for s in SOURCES]
+    res = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp] + objs,
+                         capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stderr[-4000:]}")
-    if verbose:
-        print(res.stderr[-2000:])
+        raise RuntimeError(f"link failed ({res.returncode}):\n{res.stderr[-4000:]}")
     os.replace(tmp, LIB)
     return LIB
 

@@ -25,9 +25,11 @@ namespace qedf {
 //   (M^dag M x)_t: y = M x is produced slice by slice in registers and M^dag
 //                  applied to it, so x is read once and one extra slice of y
 //                  (the slab's lower halo) is recomputed.
-template <typename R, typename A, int BY, int OP, bool PHS>
+template <typename R, typename A, int BY, int OP, int EC>
 __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_operator(OpArgs p) {
   extern __shared__ __align__(16) unsigned char smem[];
+  constexpr bool PHS = (EC & EC_PHS) != 0;
+  constexpr bool STASH = (EC & EC_NOSTASH) == 0;
   Slice<R, BY, PHS> S;
   S.init(p.L, smem, 2, (R)p.c1, (R)p.ch, threadIdx.x);
   const int Vs = p.L * p.L;
@@ -40,8 +42,10 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_operator(OpArgs p)
   R* z = reinterpret_cast<R*>(p.z) + (size_t)rb * p.Nt * sv;
   const R t1 = (R)p.t1, th = (R)p.th, Cb = (R)p.Cb;
   const int Nt = p.Nt;
-  // Three blocks live in registers; y_t waits in the thread-private stash.
+  // Three blocks live in registers; y_t waits in the thread-private stash
+  // (or in a fourth register block when there is no stash).
   Cx<R> X0[BY][2], X1[BY][2], Y[BY][2];
+  Cx<R> Yp[STASH ? 1 : BY][2];
 
   if (OP == OP_M) {
     int tp = (a - 1 + Nt) % Nt;
@@ -81,7 +85,7 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_operator(OpArgs p)
     S.phases(phi + tp * sv, t1, th);
     S.template applyB<FAC_TILDE>(X0);
     axpy_blk<R, BY>(Y, X1, sigma_of<R>(tp, Nt) * Cb, X0);
-    S.park(Y);
+    if constexpr (STASH) S.park(Y); else copy_blk<R, BY>(Yp, Y);
     copy_blk<R, BY>(X0, X1);
     for (int t = a; t < b; ++t) {
       const int tn = (t + 1) % Nt;
@@ -90,8 +94,13 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_operator(OpArgs p)
       const R sg = sigma_of<R>(t, Nt) * Cb;
       S.template applyB<FAC_TILDE>(X0);          // B_t x_t
       axpy_blk<R, BY>(Y, X1, sg, X0);             // y_{t+1}
-      S.unpark(X0);                               // y_t
-      S.park(Y);
+      if constexpr (STASH) {
+        S.unpark(X0);                             // y_t
+        S.park(Y);
+      } else {
+        copy_blk<R, BY>(X0, Yp);
+        copy_blk<R, BY>(Yp, Y);
+      }
       S.template applyB<FAC_TILDE>(Y);            // B_t y_{t+1}
       if (S.on) {
         axpy_blk<R, BY>(Y, X0, sg, Y);            // z_t = y_t - sigma_t B_t y_{t+1}
@@ -547,31 +556,33 @@ int pick_by(int L, int requested, int real_bytes) {
 
 static size_t smem_limit() { return 227 * 1024; }
 
-template <typename R, typename A, int BY, bool PHS>
+template <typename R, typename A, int BY, int EC>
 static int launch_operator_t(int op, const OpArgs& a, cudaStream_t st) {
   const int threads = ((a.L / 2) * (a.L / BY) + 31) / 32 * 32;
-  const size_t smem = slice_smem_bytes<R, PHS>(a.L, BY, 2);
+  const size_t smem = slice_smem_bytes<R, EC>(a.L, BY, 2);
   if (smem > smem_limit()) return QEDF_ERR_SIZE;
   dim3 grid((a.Nt + a.T - 1) / a.T, a.bs);
   if (op == OP_M) {
-    if (prepare_smem(k_operator<R, A, BY, OP_M, PHS>, smem)) return QEDF_ERR_CUDA;
-    k_operator<R, A, BY, OP_M, PHS><<<grid, threads, smem, st>>>(a);
+    if (prepare_smem(k_operator<R, A, BY, OP_M, EC>, smem)) return QEDF_ERR_CUDA;
+    k_operator<R, A, BY, OP_M, EC><<<grid, threads, smem, st>>>(a);
   } else if (op == OP_MH) {
-    if (prepare_smem(k_operator<R, A, BY, OP_MH, PHS>, smem)) return QEDF_ERR_CUDA;
-    k_operator<R, A, BY, OP_MH, PHS><<<grid, threads, smem, st>>>(a);
+    if (prepare_smem(k_operator<R, A, BY, OP_MH, EC>, smem)) return QEDF_ERR_CUDA;
+    k_operator<R, A, BY, OP_MH, EC><<<grid, threads, smem, st>>>(a);
   } else {
-    if (prepare_smem(k_operator<R, A, BY, OP_MHM, PHS>, smem)) return QEDF_ERR_CUDA;
-    k_operator<R, A, BY, OP_MHM, PHS><<<grid, threads, smem, st>>>(a);
+    if (prepare_smem(k_operator<R, A, BY, OP_MHM, EC>, smem)) return QEDF_ERR_CUDA;
+    k_operator<R, A, BY, OP_MHM, EC><<<grid, threads, smem, st>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
 
-// double precision keeps the phases in shared memory when they fit
+// double precision keeps the phases in shared memory when they fit; without
+// room for the stash, y stays in registers
 template <typename R, typename A, int BY>
 static int launch_operator_by(int op, const OpArgs& a, cudaStream_t st) {
-  if (sizeof(R) == 8 && slice_smem_bytes<R, true>(a.L, BY, 2) <= smem_limit())
-    return launch_operator_t<R, A, BY, true>(op, a, st);
-  return launch_operator_t<R, A, BY, false>(op, a, st);
+  if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
+    return launch_operator_t<R, A, BY, EC_PHS>(op, a, st);
+  if (slice_smem_bytes<R, 0>(a.L, BY, 2) <= smem_limit()) return launch_operator_t<R, A, BY, 0>(op, a, st);
+  return launch_operator_t<R, A, BY, EC_NOSTASH>(op, a, st);
 }
 
 template <typename R, typename A>
@@ -597,7 +608,7 @@ template int launch_operator<double, double>(int, OpArgs, int, cudaStream_t);
 template <typename R, typename A, int BY>
 static int launch_bvec_by(const BvecArgs& a, int nvec, cudaStream_t st) {
   const int threads = ((a.L / 2) * (a.L / BY) + 31) / 32 * 32;
-  const size_t smem = slice_smem_bytes<R, false>(a.L, BY, 2);
+  const size_t smem = slice_smem_bytes<R, 0>(a.L, BY, 2);
   if (smem > smem_limit()) return QEDF_ERR_SIZE;
   if (prepare_smem(k_bvec<R, A, BY, false>, smem)) return QEDF_ERR_CUDA;
   k_bvec<R, A, BY, false><<<nvec, threads, smem, st>>>(a);
@@ -631,7 +642,7 @@ template int launch_precon<double>(const PreconArgs&, cudaStream_t);
 template <typename R, typename A, int BY, bool PHS>
 static int launch_force_t(const ForceArgs& a, cudaStream_t st) {
   const int threads = ((a.L / 2) * (a.L / BY) + 31) / 32 * 32;
-  const size_t smem = slice_smem_bytes<R, PHS>(a.L, BY, 4);
+  const size_t smem = slice_smem_bytes<R, PHS ? EC_PHS : 0>(a.L, BY, 4);
   if (smem > smem_limit()) return QEDF_ERR_SIZE;
   if (prepare_smem(k_force<R, A, BY, PHS>, smem)) return QEDF_ERR_CUDA;
   dim3 grid((a.Nt + a.T - 1) / a.T, a.bs);
@@ -641,7 +652,7 @@ static int launch_force_t(const ForceArgs& a, cudaStream_t st) {
 
 template <typename R, typename A, int BY>
 static int launch_force_by(const ForceArgs& a, cudaStream_t st) {
-  if (sizeof(R) == 8 && slice_smem_bytes<R, true>(a.L, BY, 4) <= smem_limit())
+  if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS>(a.L, BY, 4) <= smem_limit())
     return launch_force_t<R, A, BY, true>(a, st);
   return launch_force_t<R, A, BY, false>(a, st);
 }

@@ -156,8 +156,10 @@ struct RhsState {
 // ---------------------------------------------------------------------------
 // the persistent kernel
 // ---------------------------------------------------------------------------
-template <typename RS, typename RH, typename A, int BY, bool PHS_S, bool PHS_H>
+template <typename RS, typename RH, typename A, int BY, int ECS, int ECH>
 __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_constant__ PcgParams p) {
+  constexpr bool PHS_S = (ECS & EC_PHS) != 0, STASH_S = (ECS & EC_NOSTASH) == 0;
+  constexpr bool PHS_H = (ECH & EC_PHS) != 0, STASH_H = (ECH & EC_NOSTASH) == 0;
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ RhsState st;
   constexpr bool MIXED = !std::is_same<RS, RH>::value;
@@ -312,6 +314,7 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     RS* O = Op + vb;
     const RS t1 = (RS)p.t1, th = (RS)p.th, Cb = (RS)p.Cb;
     Cx<RS> X0[BY][2], X1[BY][2], Y[BY][2];
+    Cx<RS> Yp[STASH_S ? 1 : BY][2];
     double pap = 0;
     auto getp = [&](Cx<RS> (&X)[BY][2], int t) {
       if (!E.on) return;
@@ -335,7 +338,7 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     E.phases(phi + tp * sv, t1, th);
     E.template applyB<FAC_TILDE>(X0);
     axpy_blk<RS, BY>(Y, X1, sigma_of<RS>(tp, Nt) * Cb, X0);  // y_a
-    E.park(Y);
+    if constexpr (STASH_S) E.park(Y); else copy_blk<RS, BY>(Yp, Y);
     copy_blk<RS, BY>(X0, X1);
     for (int t = a; t < bnd; ++t) {
       const int tn = (t + 1) % Nt;
@@ -345,8 +348,13 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
       const RS sg = sigma_of<RS>(t, Nt) * Cb;
       E.template applyB<FAC_TILDE>(X0);       // B_t p_t
       axpy_blk<RS, BY>(Y, X1, sg, X0);         // y_{t+1}
-      E.unpark(X0);                            // y_t
-      E.park(Y);
+      if constexpr (STASH_S) {
+        E.unpark(X0);                          // y_t
+        E.park(Y);
+      } else {
+        copy_blk<RS, BY>(X0, Yp);
+        copy_blk<RS, BY>(Yp, Y);
+      }
       if (E.on) {
 #pragma unroll
         for (int q = 0; q < BY; ++q)
@@ -384,6 +392,7 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     RS* rout = r + vb;
     const RH t1 = (RH)p.t1, th = (RH)p.th, Cb = (RH)p.Cb;
     Cx<RH> X0[BY][2], X1[BY][2], Y[BY][2];
+    Cx<RH> Yp[STASH_H ? 1 : BY][2];
     double rr_acc = 0;
     const int tp = (a - 1 + Nt) % Nt;
     if (E.on) {
@@ -393,7 +402,7 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     E.phases(phi + tp * sv, t1, th);
     E.template applyB<FAC_TILDE>(X0);
     axpy_blk<RH, BY>(Y, X1, sigma_of<RH>(tp, Nt) * Cb, X0);
-    E.park(Y);
+    if constexpr (STASH_H) E.park(Y); else copy_blk<RH, BY>(Yp, Y);
     copy_blk<RH, BY>(X0, X1);
     for (int t = a; t < bnd; ++t) {
       const int tn = (t + 1) % Nt;
@@ -402,8 +411,13 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
       const RH sg = sigma_of<RH>(t, Nt) * Cb;
       E.template applyB<FAC_TILDE>(X0);
       axpy_blk<RH, BY>(Y, X1, sg, X0);
-      E.unpark(X0);
-      E.park(Y);
+      if constexpr (STASH_H) {
+        E.unpark(X0);
+        E.park(Y);
+      } else {
+        copy_blk<RH, BY>(X0, Yp);
+        copy_blk<RH, BY>(Yp, Y);
+      }
       E.template applyB<FAC_TILDE>(Y);
       if (E.on) {
         axpy_blk<RH, BY>(Y, X0, sg, Y);  // (A x)_t
@@ -669,7 +683,7 @@ size_t pcg_workspace_bytes(const PcgParams& p, int sloppy_bytes) {
   return nv * vecb + accb + 256;
 }
 
-template <typename RS, typename RH, typename A, int BY, bool PHS_S, bool PHS_H>
+template <typename RS, typename RH, typename A, int BY, int ECS, int ECH>
 static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   int Lmax = 0, Ntmax = 0;
   for (int s = 0; s < p.nsys; ++s) {
@@ -680,11 +694,11 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   const int eng_threads = (Lmax / 2) * (Lmax / BY);
   if (eng_threads > MaxThreads<BY>::value) return QEDF_ERR_SIZE;
   const int threads = std::min(MaxThreads<BY>::value, std::max(128, (eng_threads + 31) / 32 * 32));
-  size_t smem = slice_smem_bytes<RS, PHS_S>(Lmax, BY, 2);
-  smem = std::max(smem, slice_smem_bytes<RH, PHS_H>(Lmax, BY, 2));
+  size_t smem = slice_smem_bytes<RS, ECS>(Lmax, BY, 2);
+  smem = std::max(smem, slice_smem_bytes<RH, ECH>(Lmax, BY, 2));
   smem = std::max(smem, sizeof(Cx<RS>) * (size_t)Ntmax * p.CH);
   if (smem + sizeof(RhsState) > 227 * 1024) return QEDF_ERR_SIZE;
-  auto kern = k_pcg<RS, RH, A, BY, PHS_S, PHS_H>;
+  auto kern = k_pcg<RS, RH, A, BY, ECS, ECH>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return QEDF_ERR_CUDA;
   int per_sm = 0;
@@ -705,33 +719,29 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   return QEDF_OK;
 }
 
-static size_t pcg_fixed_smem(const PcgParams& p, int real_bytes, int& Lmax) {
-  int Ntmax = 0;
-  Lmax = 0;
-  for (int s = 0; s < p.nsys; ++s) {
-    Lmax = std::max(Lmax, p.sys[s].L);
-    Ntmax = std::max(Ntmax, p.sys[s].Nt);
-  }
-  return (size_t)real_bytes * 2 * Ntmax * p.CH + sizeof(RhsState);
-}
+static bool fits(size_t engine_bytes) { return engine_bytes + sizeof(RhsState) <= 227 * 1024; }
 
 template <int BY>
 static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
   int Lmax = 0;
+  for (int s = 0; s < p.nsys; ++s) Lmax = std::max(Lmax, p.sys[s].L);
   switch (p.mode) {
-    case QEDF_PCG_PLAIN_F32: return launch_pcg_t<float, float, float, BY, false, false>(p, st);
-    case QEDF_PCG_PLAIN_F64: {
-      pcg_fixed_smem(p, 8, Lmax);
-      if (slice_smem_bytes<double, true>(Lmax, BY, 2) + sizeof(RhsState) <= 227 * 1024)
-        return launch_pcg_t<double, double, double, BY, true, true>(p, st);
-      return launch_pcg_t<double, double, double, BY, false, false>(p, st);
-    }
-    case QEDF_PCG_MIXED: {
-      pcg_fixed_smem(p, 4, Lmax);
-      if (slice_smem_bytes<double, true>(Lmax, BY, 2) + sizeof(RhsState) <= 227 * 1024)
-        return launch_pcg_t<float, double, float, BY, false, true>(p, st);
-      return launch_pcg_t<float, double, float, BY, false, false>(p, st);
-    }
+    case QEDF_PCG_PLAIN_F32:
+      if (fits(slice_smem_bytes<float, 0>(Lmax, BY, 2)))
+        return launch_pcg_t<float, float, float, BY, 0, 0>(p, st);
+      return launch_pcg_t<float, float, float, BY, EC_NOSTASH, EC_NOSTASH>(p, st);
+    case QEDF_PCG_PLAIN_F64:
+      if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
+        return launch_pcg_t<double, double, double, BY, EC_PHS, EC_PHS>(p, st);
+      if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
+        return launch_pcg_t<double, double, double, BY, 0, 0>(p, st);
+      return launch_pcg_t<double, double, double, BY, EC_NOSTASH, EC_NOSTASH>(p, st);
+    case QEDF_PCG_MIXED:
+      if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
+        return launch_pcg_t<float, double, float, BY, 0, EC_PHS>(p, st);
+      if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
+        return launch_pcg_t<float, double, float, BY, 0, 0>(p, st);
+      return launch_pcg_t<float, double, float, BY, 0, EC_NOSTASH>(p, st);
   }
   return QEDF_ERR_ARG;
 }

@@ -40,11 +40,18 @@ struct MaxThreads {
 // thread's own bond phases in registers and only the neighbours' in shared
 // memory; PHS = true (used in double precision to relieve registers) keeps
 // the phases of all 2 Vs bonds of the slice in shared memory.
-template <typename R, bool PHS = false>
+//
+// Engine configuration bits (template parameter EC of the kernels):
+//   EC_PHS     phases of all bonds in shared memory (else own ones in registers)
+//   EC_NOSTASH no shared-memory stash: the previous y block stays in registers
+// (used only where the shared memory of the default layout does not fit).
+enum { EC_PHS = 1, EC_NOSTASH = 2 };
+
+template <typename R, int EC = 0>
 __host__ __device__ inline size_t slice_smem_bytes(int L, int BY, int nbuf) {
   const size_t Vs = (size_t)L * L;
-  const size_t ph = PHS ? 2 * Vs : Vs / 2 + Vs / BY;
-  return sizeof(Cx<R>) * (nbuf * Vs + ph + Vs);
+  const size_t ph = (EC & EC_PHS) ? 2 * Vs : Vs / 2 + Vs / BY;
+  return sizeof(Cx<R>) * (nbuf * Vs + ph + ((EC & EC_NOSTASH) ? 0 : Vs));
 }
 
 template <typename R, int BY, bool PHS = false>
