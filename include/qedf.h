@@ -181,6 +181,10 @@ typedef struct {
   double ru_delta;    /* mixed: and whenever the residual fell by this factor */
   int by, slab, chunk;/* tile choice, 0 = automatic */
   double timeout_ms;  /* per grid-barrier wait, 0 = 2000 ms */
+  long long* profile; /* optional device array of 8 counters (zeroed by the caller) that
+                         accumulate SM clock cycles of block 0: 0 init, 1 operator phases,
+                         2 waits after them, 3 elementwise phases, 4 waits after them,
+                         5 reliable updates, 6 per-iteration bookkeeping, 7 whole solve */
 } qedf_pcg_opts;
 
 /* Bytes of device workspace qedf_pcg_solve needs for these systems. */

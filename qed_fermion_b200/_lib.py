@@ -44,6 +44,7 @@ class QedfPcgOpts(ctypes.Structure):
         ("slab", c_int),
         ("chunk", c_int),
         ("timeout_ms", c_double),
+        ("profile", c_void_p),
     ]
 
 
@@ -109,7 +110,8 @@ def call(name, *args):
     lib = load()
     st = getattr(lib, name)(*args)
     if name not in _HOST_ONLY:
-        LAUNCHES["count"] += 1
+        # qedf_pcg_solve launches a small preparation kernel and the solver
+        LAUNCHES["count"] += 2 if name == "qedf_pcg_solve" else 1
     if st != QEDF_OK:
         raise QedfError(name, st, lib.qedf_status_string(st).decode())
     return st

@@ -1,6 +1,7 @@
 // extern "C" entry points declared in include/qedf.h: argument validation on
 // the host, then the kernel launchers of qedf_ops.cu / qedf_pcg.cu.
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 
 #include "qedf_common.cuh"
@@ -37,6 +38,7 @@ int op_entry(int op, const A* boson, const R* x, R* out, int bs, int Lx, int Lta
   a.bs = bs;
   a.rhs_per_phi = rhs_per_boson;
   a.T = slab;
+  a.xs = std::getenv("QEDF_NO_XS") ? 0 : 1;  // tuning switch: warp-shuffle engine off
   a.c1 = f.c1;
   a.ch = f.ch;
   a.t1 = f.t1;
@@ -304,12 +306,15 @@ int qedf_pcg_solve(const qedf_system* sys, int nsys, const void* boson, const vo
   const size_t accb = ((sizeof(double) * 9 * p.nrhs) + 255) / 256 * 256;
   off += accb;
   p.bar = reinterpret_cast<unsigned int*>(w + off);
+  off += 256;
+  p.ptab = reinterpret_cast<float*>(w + off);
   p.phi = boson;
   p.b = b;
   p.x = x;
   p.iters = iters;
   p.relres = relres;
   p.status = status;
+  p.prof = opts->profile;
   const double tmo = opts->timeout_ms > 0 ? opts->timeout_ms : 2000.0;
   int dev = 0, clk_khz = 0;
   cudaGetDevice(&dev);
@@ -317,8 +322,8 @@ int qedf_pcg_solve(const qedf_system* sys, int nsys, const void* boson, const vo
   if (clk_khz <= 0) clk_khz = 2000000;
   p.timeout_cycles = (long long)(tmo * (double)clk_khz);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  // accumulators and barrier state start at zero
-  if (cudaMemsetAsync(p.acc, 0, accb + 256, st) != cudaSuccess) return QEDF_ERR_CUDA;
+  // accumulators and barrier state start at zero; preconditioner tables
+  if (int e2 = launch_pcg_prep(p, (int)((accb + 256) / 4), st)) return e2;
   return launch_pcg(p, opts->by, st);
 }
 

@@ -17,6 +17,7 @@ struct OpArgs {
   int L, Nt, bs;
   int rhs_per_phi;  // consecutive vectors sharing one angle array
   int T;            // slab length (0 = auto)
+  int xs;           // allow the warp-shuffle engine (single precision, L <= 64)
   double c1, ch, t1, th, Cb;
 };
 
@@ -88,6 +89,7 @@ int launch_cdot(const R* u, const R* v, int64_t n, int rows, double* out, cudaSt
 // ---- persistent PCG -------------------------------------------------------
 constexpr int PCG_MAX_SYS = 32;
 constexpr int PCG_MAX_RHS = 256;
+constexpr int PCG_CHUNK = 16;  // sites per elementwise unit (a multiple of 2)
 
 struct PcgSys {
   int L, Nt, nrhs, shared;
@@ -98,12 +100,14 @@ struct PcgSys {
   int64_t vec0;          // first complex element of the system in the packed vectors
   int64_t phi0;          // first real of the system in the packed angles
   int precon;
+  int ptab0;             // first entry of the system's preconditioner band table
 };
 
 struct PcgParams {
   int nsys, nrhs, unitsA, unitsE, CH;
   PcgSys sys[PCG_MAX_SYS];
   int mode;  // QEDF_PCG_PLAIN_F32, QEDF_PCG_PLAIN_F64, QEDF_PCG_MIXED
+  int xs;    // allow the warp-shuffle engine for the single-precision iterations
   int max_iter, ru_interval;
   double rtol, ru_delta;
   double c1, ch, t1, th, Cb;
@@ -120,15 +124,19 @@ struct PcgParams {
   void* Op;
   void* xlo;         // mixed only
   double* acc;       // accumulators
+  float* ptab;       // periodic 13-band tau tables of the preconditioner, per system
   unsigned int* bar; // [0] count, [1] generation, [2] error
   int* iters;
   double* relres;
   int* status;
   int64_t nvec_total;  // complex elements per vector buffer
+  int ptab_len;        // floats of all preconditioner tables
+  long long* prof;     // optional [8] cycle counters of block 0 (see k_pcg), or null
 };
 
 size_t pcg_workspace_bytes(const PcgParams& p, int sloppy_bytes);
 int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts* o);
 int launch_pcg(PcgParams& p, int by, cudaStream_t st);
+int launch_pcg_prep(const PcgParams& p, int zero_words, cudaStream_t st);
 
 }  // namespace qedf

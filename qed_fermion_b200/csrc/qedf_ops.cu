@@ -26,11 +26,12 @@ namespace qedf {
 //                  applied to it, so x is read once and one extra slice of y
 //                  (the slab's lower halo) is recomputed.
 template <typename R, typename A, int BY, int OP, int EC>
-__global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_operator(OpArgs p) {
+__global__ void __launch_bounds__(MaxT<BY, EC>::value, 1) k_operator(OpArgs p) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr bool PHS = (EC & EC_PHS) != 0;
   constexpr bool STASH = (EC & EC_NOSTASH) == 0;
-  Slice<R, BY, PHS> S;
+  constexpr bool XS = (EC & EC_XS) != 0;
+  Slice<R, BY, PHS, XS> S;
   S.init(p.L, smem, 2, (R)p.c1, (R)p.ch, threadIdx.x);
   const int Vs = p.L * p.L;
   const size_t sv = 2 * (size_t)Vs;  // reals per slice (vector and angles)
@@ -82,6 +83,8 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_operator(OpArgs p)
       S.load(X0, x + tp * sv);
       S.load(X1, x + a * sv);
     }
+    A ang[BY][4];
+    if constexpr (!PHS) S.load_angles(ang, phi + a * sv);
     S.phases(phi + tp * sv, t1, th);
     S.template applyB<FAC_TILDE>(X0);
     axpy_blk<R, BY>(Y, X1, sigma_of<R>(tp, Nt) * Cb, X0);
@@ -90,7 +93,13 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_operator(OpArgs p)
     for (int t = a; t < b; ++t) {
       const int tn = (t + 1) % Nt;
       if (S.on) S.load(X1, x + tn * sv);
-      S.phases(phi + t * sv, t1, th);
+      if constexpr (!PHS) {
+        // phases of slice t from angles fetched one slice ahead
+        S.phases_from(ang, t1, th);
+        if (t + 1 < b) S.load_angles(ang, phi + (t + 1) * sv);
+      } else {
+        S.phases(phi + t * sv, t1, th);
+      }
       const R sg = sigma_of<R>(t, Nt) * Cb;
       S.template applyB<FAC_TILDE>(X0);          // B_t x_t
       axpy_blk<R, BY>(Y, X1, sg, X0);             // y_{t+1}
@@ -558,9 +567,9 @@ static size_t smem_limit() { return 227 * 1024; }
 
 template <typename R, typename A, int BY, int EC>
 static int launch_operator_t(int op, const OpArgs& a, cudaStream_t st) {
-  const int threads = ((a.L / 2) * (a.L / BY) + 31) / 32 * 32;
+  const int threads = slice_threads(a.L, BY, (EC & EC_XS) != 0);
   const size_t smem = slice_smem_bytes<R, EC>(a.L, BY, 2);
-  if (smem > smem_limit()) return QEDF_ERR_SIZE;
+  if (smem > smem_limit() || threads > MaxT<BY, EC>::value) return QEDF_ERR_SIZE;
   dim3 grid((a.Nt + a.T - 1) / a.T, a.bs);
   if (op == OP_M) {
     if (prepare_smem(k_operator<R, A, BY, OP_M, EC>, smem)) return QEDF_ERR_CUDA;
@@ -578,9 +587,12 @@ static int launch_operator_t(int op, const OpArgs& a, cudaStream_t st) {
 // double precision keeps the phases in shared memory when they fit; without
 // room for the stash, y stays in registers
 template <typename R, typename A, int BY>
-static int launch_operator_by(int op, const OpArgs& a, cudaStream_t st) {
+static int launch_operator_by(int op, const OpArgs& a, int xs, cudaStream_t st) {
   if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
     return launch_operator_t<R, A, BY, EC_PHS>(op, a, st);
+  if (sizeof(R) == 4 && xs && xs_possible(a.L) && ((a.L / 2) & (a.L / 2 - 1)) == 0 &&
+      slice_threads(a.L, BY, true) <= MaxT<BY, EC_XS>::value)
+    return launch_operator_t<R, A, BY, EC_XS>(op, a, st);
   if (slice_smem_bytes<R, 0>(a.L, BY, 2) <= smem_limit()) return launch_operator_t<R, A, BY, 0>(op, a, st);
   return launch_operator_t<R, A, BY, EC_NOSTASH>(op, a, st);
 }
@@ -595,10 +607,11 @@ int launch_operator(int op, OpArgs a, int by, cudaStream_t st) {
     long slabs = std::max(1L, want / std::max(1, a.bs));
     a.T = (int)std::max(1L, (a.Nt + slabs - 1) / slabs);
   }
+  const int xs = a.xs;
   switch (by) {
-    case 2: return launch_operator_by<R, A, 2>(op, a, st);
-    case 4: return launch_operator_by<R, A, 4>(op, a, st);
-    case 6: return launch_operator_by<R, A, 6>(op, a, st);
+    case 2: return launch_operator_by<R, A, 2>(op, a, xs, st);
+    case 4: return launch_operator_by<R, A, 4>(op, a, xs, st);
+    case 6: return launch_operator_by<R, A, 6>(op, a, xs, st);
   }
   return QEDF_ERR_ARG;
 }

@@ -153,12 +153,34 @@ struct RhsState {
   double red[32];
 };
 
+// Optional phase timing (block 0, thread 0): prof[k] accumulates clock64 cycles of
+//   0 init, 1 operator phase work, 2 wait after it, 3 elementwise phase work,
+//   4 wait after it, 5 reliable updates (work + waits), 6 iterations, 7 total
+struct PhaseClock {
+  long long* prof;
+  long long t;
+  __device__ PhaseClock(long long* p) : prof((p && blockIdx.x == 0 && threadIdx.x == 0) ? p : nullptr), t(0) {
+    if (prof) t = clock64();
+  }
+  __device__ __forceinline__ void lap(int k) {
+    if (prof) {
+      const long long n = clock64();
+      prof[k] += n - t;
+      t = n;
+    }
+  }
+  __device__ __forceinline__ void add(int k, long long v) {
+    if (prof) prof[k] += v;
+  }
+};
+
 // ---------------------------------------------------------------------------
 // the persistent kernel
 // ---------------------------------------------------------------------------
 template <typename RS, typename RH, typename A, int BY, int ECS, int ECH>
-__global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_constant__ PcgParams p) {
+__global__ void __launch_bounds__(MaxT<BY, ECS>::value, 1) k_pcg(const __grid_constant__ PcgParams p) {
   constexpr bool PHS_S = (ECS & EC_PHS) != 0, STASH_S = (ECS & EC_NOSTASH) == 0;
+  constexpr bool XS_S = (ECS & EC_XS) != 0;
   constexpr bool PHS_H = (ECH & EC_PHS) != 0, STASH_H = (ECH & EC_NOSTASH) == 0;
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ RhsState st;
@@ -175,7 +197,9 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
   RH* xh = reinterpret_cast<RH*>(p.x);
   const RH* bvec = reinterpret_cast<const RH*>(p.b);
   const A* phi_all = reinterpret_cast<const A*>(p.phi);
-  const int CH = p.CH;
+  constexpr int CH = PCG_CHUNK;   // sites per elementwise unit
+  constexpr int CHC = PCG_CHUNK;
+  constexpr int PPR = CHC / 2;    // site pairs per row of a unit
 
   for (int v = tid; v < NV; v += blockDim.x) {
     st.active[v] = 1;
@@ -204,7 +228,12 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
 
   // ---- BC-type elementwise pass over one unit --------------------------------
   // kind 0: init (x = 0, r = b, bb); 1: iteration update; 2: preconditioner only
-  // (after a reliable update).  Leaves r of the chunk in smem, applies P.
+  // (after a reliable update).  A unit is CHC sites of one right-hand side over
+  // all tau; a thread handles two neighbouring sites (one 16-byte access per
+  // vector in single precision) in every (blockDim/PPR)-th row.  r of the unit
+  // stays in shared memory for the tau-stencil of the preconditioner, whose
+  // periodic 13-band table P_tab[t][k] (offset k - 6; the corners of the
+  // reference's matrix are the band's wrap-around) was prepared per system.
   auto elementwise = [&](int kind, int u, int slot) {
     int s, v, c0, c1;
     unitE(u, s, v, c0, c1);
@@ -214,74 +243,79 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     Cx<RS>* rsm = reinterpret_cast<Cx<RS>*>(dsm);
     const RS al = (RS)st.alpha[v];
     const RS* pn = reinterpret_cast<const RS*>((st.iters[v] & 1) ? p.p1 : p.p0);
-    double acc_a = 0, acc_b = 0;
-    for (int e = tid; e < Nt * CH; e += blockDim.x) {
-      const int t = e / CH, j = e % CH;
-      if (j >= w) continue;
-      const int64_t i = base + (int64_t)t * Vs + c0 + j;
-      Cx<RS> rv;
+    const RS* opv = reinterpret_cast<const RS*>(Op);
+    const int j = tid % PPR;
+    const int rstep = blockDim.x / PPR;
+    const bool jon = 2 * j < w;
+    double acc_a = 0, acc_b = 0, acc_c = 0;
+#pragma unroll 2
+    for (int t = tid / PPR; t < Nt; t += rstep) {
+      if (!jon) continue;
+      const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);  // reals
+      Cx<RS> r0, r1;
       if (kind == 0) {
-        const Cx<RH> bv = ldc(bvec, i);
-        acc_a += (double)bv.re * bv.re + (double)bv.im * bv.im;  // bb
-        rv = mk<RS>((RS)bv.re, (RS)bv.im);
-        stc(xs, i, mk<RS>(0, 0));
-        if (MIXED) stc(xh, i, mk<RH>(0, 0));
-        stc(r, i, rv);
+        Cx<RH> b0, b1;
+        ld2c(bvec + i2, b0, b1);
+        acc_a += (double)b0.re * b0.re + (double)b0.im * b0.im + (double)b1.re * b1.re + (double)b1.im * b1.im;
+        r0 = mk<RS>((RS)b0.re, (RS)b0.im);
+        r1 = mk<RS>((RS)b1.re, (RS)b1.im);
+        st2(xs + i2, mk<RS>(0, 0), mk<RS>(0, 0));
+        if (MIXED) st2(xh + i2, mk<RH>(0, 0), mk<RH>(0, 0));
+        st2(r + i2, r0, r1);
       } else if (kind == 1) {
-        const Cx<RS> pv = ldc(pn, i), ov = ldc(reinterpret_cast<const RS*>(Op), i);
-        Cx<RS> xv = ldc(reinterpret_cast<const RS*>(xs), i);
-        rv = ldc(reinterpret_cast<const RS*>(r), i);
-        xv = mk<RS>(fma(al, pv.re, xv.re), fma(al, pv.im, xv.im));
-        rv = mk<RS>(fma(-al, ov.re, rv.re), fma(-al, ov.im, rv.im));
-        stc(xs, i, xv);
-        stc(r, i, rv);
+        Cx<RS> p0v, p1v, o0, o1, x0, x1;
+        ld2c(pn + i2, p0v, p1v);
+        ld2c(opv + i2, o0, o1);
+        ld2c(xs + i2, x0, x1);
+        ld2c(r + i2, r0, r1);
+        x0 = mk<RS>(fma(al, p0v.re, x0.re), fma(al, p0v.im, x0.im));
+        x1 = mk<RS>(fma(al, p1v.re, x1.re), fma(al, p1v.im, x1.im));
+        r0 = mk<RS>(fma(-al, o0.re, r0.re), fma(-al, o0.im, r0.im));
+        r1 = mk<RS>(fma(-al, o1.re, r1.re), fma(-al, o1.im, r1.im));
+        st2(xs + i2, x0, x1);
+        st2(r + i2, r0, r1);
       } else {
-        rv = ldc(reinterpret_cast<const RS*>(r), i);
+        ld2c(r + i2, r0, r1);
       }
-      if (kind != 0) acc_a += (double)rv.re * rv.re + (double)rv.im * rv.im;  // rr
-      rsm[t * CH + j] = rv;
+      acc_c += (double)r0.re * r0.re + (double)r0.im * r0.im + (double)r1.re * r1.re + (double)r1.im * r1.im;
+      st2(reinterpret_cast<RS*>(rsm + t * CHC + 2 * j), r0, r1);
     }
     __syncthreads();
-    for (int e = tid; e < Nt * CH; e += blockDim.x) {
-      const int t = e / CH, j = e % CH;
-      if (j >= w) continue;
-      const int64_t i = base + (int64_t)t * Vs + c0 + j;
-      const Cx<RS> rv = rsm[t * CH + j];
-      Cx<RS> zv;
+    const float* tab = p.ptab + S.ptab0;
+#pragma unroll 2
+    for (int t = tid / PPR; t < Nt; t += rstep) {
+      if (!jon) continue;
+      Cx<RS> r0, r1;
+      ld2c(reinterpret_cast<const RS*>(rsm + t * CHC + 2 * j), r0, r1);
+      Cx<RS> z0 = r0, z1 = r1;
       if (S.precon) {
-        RS zr = 0, zi = 0;
-        pre_row(c_pre, Nt, t, [&](int col, float val) {
-          const Cx<RS> q = rsm[col * CH + j];
-          zr = fma((RS)val, q.re, zr);
-          zi = fma((RS)val, q.im, zi);
-        });
-        zv = mk<RS>(zr, zi);
-        stc(z, i, zv);
-      } else {
-        zv = rv;
+        z0 = mk<RS>(0, 0);
+        z1 = mk<RS>(0, 0);
+        int tt = t - 6 < 0 ? t - 6 + Nt : t - 6;
+#pragma unroll
+        for (int k = 0; k < 13; ++k) {
+          const RS c = (RS)__ldg(tab + t * 13 + k);
+          Cx<RS> q0, q1;
+          ld2c(reinterpret_cast<const RS*>(rsm + tt * CHC + 2 * j), q0, q1);
+          z0 = mk<RS>(fma(c, q0.re, z0.re), fma(c, q0.im, z0.im));
+          z1 = mk<RS>(fma(c, q1.re, z1.re), fma(c, q1.im, z1.im));
+          tt = tt + 1 == Nt ? 0 : tt + 1;
+        }
+        const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
+        st2(z + i2, z0, z1);
       }
-      acc_b += (double)rv.re * zv.re + (double)rv.im * zv.im;  // rz
-    }
-    // rr for init equals bb (r = b): accumulate separately
-    double rr_init = 0;
-    if (kind == 0) {
-      for (int e = tid; e < Nt * CH; e += blockDim.x) {
-        const int j = e % CH;
-        if (j >= w) continue;
-        const Cx<RS> q = rsm[e];
-        rr_init += (double)q.re * q.re + (double)q.im * q.im;
-      }
+      acc_b += (double)r0.re * z0.re + (double)r0.im * z0.im + (double)r1.re * z1.re + (double)r1.im * z1.im;
     }
     const double sa = block_sum_d(acc_a, st.red);
     const double sb = block_sum_d(acc_b, st.red);
-    const double sc = block_sum_d(rr_init, st.red);
+    const double sc = block_sum_d(acc_c, st.red);
     if (tid == 0) {
       if (kind == 0) {
         atomicAdd(acc.bb + v, sa);
         atomicAdd(acc.rr + slot * NV + v, sc);
         atomicAdd(acc.rz + slot * NV + v, sb);
       } else if (kind == 1) {
-        atomicAdd(acc.rr + slot * NV + v, sa);
+        atomicAdd(acc.rr + slot * NV + v, sc);
         atomicAdd(acc.rz + slot * NV + v, sb);
       } else {
         atomicAdd(acc.ru_rz + v, sb);
@@ -302,7 +336,7 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     const int bnd = min(a + S.T, S.Nt);
     const int Nt = S.Nt, Vs = S.L * S.L;
     const size_t sv = 2 * (size_t)Vs;
-    Slice<RS, BY, PHS_S> E;
+    Slice<RS, BY, PHS_S, XS_S> E;
     E.init(S.L, dsm, 2, (RS)p.c1, (RS)p.ch, tid);
     const int64_t vb = 2 * vec_base(s, v);  // reals
     const A* phi = phi_all + S.phi0 + (S.shared ? 0 : (int64_t)(v - S.rhs0) * Nt * sv);
@@ -335,6 +369,8 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     getp(X0, tp);
     getp(X1, a);
     if (E.on) E.store(pnew + a * sv, X1);
+    A ang[BY][4];
+    if constexpr (!PHS_S) E.load_angles(ang, phi + a * sv);
     E.phases(phi + tp * sv, t1, th);
     E.template applyB<FAC_TILDE>(X0);
     axpy_blk<RS, BY>(Y, X1, sigma_of<RS>(tp, Nt) * Cb, X0);  // y_a
@@ -344,7 +380,12 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
       const int tn = (t + 1) % Nt;
       getp(X1, tn);
       if (E.on && t + 1 < bnd) E.store(pnew + tn * sv, X1);
-      E.phases(phi + t * sv, t1, th);
+      if constexpr (!PHS_S) {
+        E.phases_from(ang, t1, th);
+        if (t + 1 < bnd) E.load_angles(ang, phi + (t + 1) * sv);
+      } else {
+        E.phases(phi + t * sv, t1, th);
+      }
       const RS sg = sigma_of<RS>(t, Nt) * Cb;
       E.template applyB<FAC_TILDE>(X0);       // B_t p_t
       axpy_blk<RS, BY>(Y, X1, sg, X0);         // y_{t+1}
@@ -448,26 +489,33 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     const PcgSys& S = p.sys[s];
     const int Vs = S.L * S.L, w = c1 - c0;
     const int64_t base = vec_base(s, v);
-    for (int e = tid; e < S.Nt * CH; e += blockDim.x) {
-      const int t = e / CH, j = e % CH;
-      if (j >= w) continue;
-      const int64_t i = base + (int64_t)t * Vs + c0 + j;
-      const Cx<RS> lo = ldc(reinterpret_cast<const RS*>(xs), i);
-      Cx<RH> hi = ldc(reinterpret_cast<const RH*>(xh), i);
-      hi.re += (RH)lo.re;
-      hi.im += (RH)lo.im;
-      stc(xh, i, hi);
-      stc(xs, i, mk<RS>(0, 0));
+    const int j = tid % PPR;
+    if (2 * j >= w) return;
+    for (int t = tid / PPR; t < S.Nt; t += blockDim.x / PPR) {
+      const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
+      Cx<RS> l0, l1;
+      Cx<RH> h0, h1;
+      ld2c(xs + i2, l0, l1);
+      ld2c(xh + i2, h0, h1);
+      h0.re += (RH)l0.re;
+      h0.im += (RH)l0.im;
+      h1.re += (RH)l1.re;
+      h1.im += (RH)l1.im;
+      st2(xh + i2, h0, h1);
+      st2(xs + i2, mk<RS>(0, 0), mk<RS>(0, 0));
     }
   };
 
   // ---------------------------------------------------------------------------
   const long long budget = p.timeout_cycles;
   bool ok = true;
+  PhaseClock pc(p.prof);
+  const long long t_begin = pc.prof ? clock64() : 0;
 
   // init: x = 0, r = b, z = P r
   for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) elementwise(0, u, 0);
   ok = grid_barrier(p.bar, nblk, budget);
+  pc.lap(0);
   int slot = 0;  // accumulator slot holding the current rr / rz
   if (ok) {
     for (int v = tid; v < NV; v += blockDim.x) {
@@ -513,6 +561,7 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     }
     __syncthreads();
     if (MIXED && st.any_ru) {
+      pc.lap(6);
       if (blockIdx.x == 0)
         for (int v = tid; v < NV; v += blockDim.x) {
           acc.ru_rr[v] = 0;
@@ -548,6 +597,7 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
         }
       }
       __syncthreads();
+      pc.lap(5);
     }
     for (int v = tid; v < NV; v += blockDim.x)
       if (st.active[v]) st.any_active = 1;
@@ -569,7 +619,9 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
         acc.rr[(slot ^ 1) * NV + v] = 0;
         acc.rz[(slot ^ 1) * NV + v] = 0;
       }
+    pc.lap(1);
     if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+    pc.lap(2);
 
     // ---- phase BC
     for (int v = tid; v < NV; v += blockDim.x) st.alpha[v] = st.rz[v] / acc.pAp[aslot * NV + v];
@@ -581,7 +633,9 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     }
     if (blockIdx.x == 0)  // pAp slot of the next iteration
       for (int v = tid; v < NV; v += blockDim.x) acc.pAp[(aslot ^ 1) * NV + v] = 0;
+    pc.lap(3);
     if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+    pc.lap(4);
     slot ^= 1;
     for (int v = tid; v < NV; v += blockDim.x) {
       if (!st.active[v]) continue;
@@ -592,6 +646,10 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_pcg(const __grid_c
     }
     __syncthreads();
     ++it;
+    pc.lap(6);
+  }
+  if (pc.prof) {
+    pc.prof[7] += clock64() - t_begin;
   }
 
   // mixed: fold the remaining float updates of unconverged systems into x
@@ -623,9 +681,11 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
     return QEDF_ERR_ARG;
   p.mode = o->mode;
   p.nsys = nsys;
-  p.CH = o->chunk > 0 ? o->chunk : 16;
+  p.xs = 1;
+  if (o->chunk != 0 && o->chunk != PCG_CHUNK) return QEDF_ERR_ARG;
+  p.CH = PCG_CHUNK;
   const int nblk = num_sms();
-  int rhs = 0, ua = 0, ue = 0;
+  int rhs = 0, ua = 0, ue = 0, pt = 0;
   int64_t vec = 0, phi = 0;
   for (int s = 0; s < nsys; ++s) {
     const qedf_system& q = sys[s];
@@ -652,6 +712,8 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
     S.unitE0 = ue;
     S.vec0 = vec;
     S.phi0 = phi;
+    S.ptab0 = pt;
+    pt += 13 * q.Ltau;
     rhs += q.nrhs;
     ua += q.nrhs * S.nslab;
     ue += q.nrhs * S.nchunk;
@@ -663,6 +725,7 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
   p.unitsA = ua;
   p.unitsE = ue;
   p.nvec_total = vec;
+  p.ptab_len = pt;
   p.max_iter = o->max_iter;
   p.rtol = o->rtol;
   p.ru_interval = o->ru_interval > 0 ? o->ru_interval : 50;
@@ -680,7 +743,36 @@ size_t pcg_workspace_bytes(const PcgParams& p, int sloppy_bytes) {
   const size_t vecb = align_up((size_t)p.nvec_total * 2 * sloppy_bytes, 256);
   const int nv = p.mode == QEDF_PCG_MIXED ? 6 : 5;
   const size_t accb = align_up(sizeof(double) * ACC_PER_RHS * p.nrhs, 256);
-  return nv * vecb + accb + 256;
+  const size_t tabb = align_up(sizeof(float) * (size_t)p.ptab_len, 256);
+  return nv * vecb + accb + 256 + tabb;
+}
+
+// Per solve: zero the accumulators and barrier words, and write each system's
+// periodic 13-band preconditioner table (entry k of row t multiplies r at
+// tau = t + k - 6 mod Nt).
+__global__ void k_pcg_prep(const __grid_constant__ PcgParams p, int zero_words) {
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned int* z = reinterpret_cast<unsigned int*>(p.acc);
+  for (int i = i0; i < zero_words; i += gridDim.x * blockDim.x) z[i] = 0u;
+  for (int s = 0; s < p.nsys; ++s) {
+    const int Nt = p.sys[s].Nt;
+    float* tab = p.ptab + p.sys[s].ptab0;
+    for (int e = i0; e < 13 * Nt; e += gridDim.x * blockDim.x) tab[e] = 0.f;
+  }
+  __syncthreads();
+  // rows are independent; each thread fills whole rows (duplicate-free)
+  for (int s = 0; s < p.nsys; ++s) {
+    const int Nt = p.sys[s].Nt;
+    if (!p.sys[s].precon) continue;
+    float* tab = p.ptab + p.sys[s].ptab0;
+    for (int t = i0; t < Nt; t += gridDim.x * blockDim.x)
+      pre_row(c_pre, Nt, t, [&](int col, float val) {
+        int k = col - t + 6;
+        if (k < 0) k += Nt;
+        if (k >= Nt) k -= Nt;
+        tab[t * 13 + k] += val;
+      });
+  }
 }
 
 template <typename RS, typename RH, typename A, int BY, int ECS, int ECH>
@@ -691,12 +783,13 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
     Ntmax = std::max(Ntmax, p.sys[s].Nt);
     if (p.sys[s].L % BY) return QEDF_ERR_ARG;
   }
-  const int eng_threads = (Lmax / 2) * (Lmax / BY);
-  if (eng_threads > MaxThreads<BY>::value) return QEDF_ERR_SIZE;
-  const int threads = std::min(MaxThreads<BY>::value, std::max(128, (eng_threads + 31) / 32 * 32));
+  int eng_threads = slice_threads(Lmax, BY, (ECS & EC_XS) != 0);
+  eng_threads = std::max(eng_threads, slice_threads(Lmax, BY, false));
+  if (eng_threads > MaxT<BY, ECS>::value) return QEDF_ERR_SIZE;
+  const int threads = std::min(MaxT<BY, ECS>::value, std::max(128, eng_threads));
   size_t smem = slice_smem_bytes<RS, ECS>(Lmax, BY, 2);
   smem = std::max(smem, slice_smem_bytes<RH, ECH>(Lmax, BY, 2));
-  smem = std::max(smem, sizeof(Cx<RS>) * (size_t)Ntmax * p.CH);
+  smem = std::max(smem, sizeof(Cx<RS>) * (size_t)Ntmax * PCG_CHUNK);
   if (smem + sizeof(RhsState) > 227 * 1024) return QEDF_ERR_SIZE;
   auto kern = k_pcg<RS, RH, A, BY, ECS, ECH>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
@@ -719,14 +812,25 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   return QEDF_OK;
 }
 
+int launch_pcg_prep(const PcgParams& p, int zero_words, cudaStream_t st) {
+  k_pcg_prep<<<1, 256, 0, st>>>(p, zero_words);
+  return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
+}
+
 static bool fits(size_t engine_bytes) { return engine_bytes + sizeof(RhsState) <= 227 * 1024; }
 
 template <int BY>
 static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
   int Lmax = 0;
   for (int s = 0; s < p.nsys; ++s) Lmax = std::max(Lmax, p.sys[s].L);
+  // the shuffle engine only pays when a row of tiles fills its warp segment
+  bool pow2 = true;
+  for (int s = 0; s < p.nsys; ++s) pow2 = pow2 && (((p.sys[s].L / 2) & (p.sys[s].L / 2 - 1)) == 0);
+  const bool xs = p.xs && pow2 && xs_possible(Lmax) && slice_threads(Lmax, BY, true) <= MaxT<BY, EC_XS>::value;
   switch (p.mode) {
     case QEDF_PCG_PLAIN_F32:
+      if (xs && fits(slice_smem_bytes<float, 0>(Lmax, BY, 2)))
+        return launch_pcg_t<float, float, float, BY, EC_XS, EC_XS>(p, st);
       if (fits(slice_smem_bytes<float, 0>(Lmax, BY, 2)))
         return launch_pcg_t<float, float, float, BY, 0, 0>(p, st);
       return launch_pcg_t<float, float, float, BY, EC_NOSTASH, EC_NOSTASH>(p, st);
@@ -737,6 +841,8 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
         return launch_pcg_t<double, double, double, BY, 0, 0>(p, st);
       return launch_pcg_t<double, double, double, BY, EC_NOSTASH, EC_NOSTASH>(p, st);
     case QEDF_PCG_MIXED:
+      if (xs && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
+        return launch_pcg_t<float, double, float, BY, EC_XS, EC_PHS>(p, st);
       if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
         return launch_pcg_t<float, double, float, BY, 0, EC_PHS>(p, st);
       if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
@@ -751,8 +857,7 @@ int launch_pcg(PcgParams& p, int by, cudaStream_t st) {
     // the tile must divide every system's L; prefer the smallest that fits
     int Lmax = 0;
     for (int s = 0; s < p.nsys; ++s) Lmax = std::max(Lmax, p.sys[s].L);
-    const int wide = p.mode == QEDF_PCG_PLAIN_F32 ? 2 : 4;
-    const int order[3] = {wide, wide == 2 ? 4 : 2, 6};
+    const int order[3] = {2, 4, 6};
     by = -1;
     for (int c : order) {
       bool ok = (Lmax / 2) * (Lmax / c) <= (c == 2 ? MaxThreads<2>::value : c == 4 ? MaxThreads<4>::value

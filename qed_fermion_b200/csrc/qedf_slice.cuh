@@ -45,7 +45,29 @@ struct MaxThreads {
 //   EC_PHS     phases of all bonds in shared memory (else own ones in registers)
 //   EC_NOSTASH no shared-memory stash: the previous y block stays in registers
 // (used only where the shared memory of the default layout does not fit).
-enum { EC_PHS = 1, EC_NOSTASH = 2 };
+//   EC_XS      exchanges of the x-bond factors by warp shuffles: a warp holds
+//              whole rows of tiles (L/2 <= 32 tiles per row, padded to a power
+//              of two), so only the y-bond factors need a block barrier
+enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4 };
+
+// Largest thread block of a kernel compiled for tile height BY and engine
+// configuration EC (it fixes the register budget: 65536 / value per thread).
+template <int BY, int EC>
+struct MaxT {
+  static constexpr int value = (EC & EC_XS) ? (BY == 2 ? 768 : (BY == 4 ? 512 : 384))
+                                            : (BY == 2 ? 576 : (BY == 4 ? 512 : 384));
+};
+
+// threads of one slice engine (a multiple of 32)
+__host__ __device__ inline int slice_threads(int L, int BY, bool xs) {
+  const int nbx = L / 2, nby = L / BY;
+  if (!xs) return (nbx * nby + 31) / 32 * 32;
+  int W = 1;
+  while (W < nbx) W <<= 1;
+  const int G = 32 / W;
+  return (nby + G - 1) / G * 32;
+}
+__host__ __device__ inline bool xs_possible(int L) { return L / 2 <= 32; }
 
 template <typename R, int EC = 0>
 __host__ __device__ inline size_t slice_smem_bytes(int L, int BY, int nbuf) {
@@ -54,10 +76,11 @@ __host__ __device__ inline size_t slice_smem_bytes(int L, int BY, int nbuf) {
   return sizeof(Cx<R>) * (nbuf * Vs + ph + ((EC & EC_NOSTASH) ? 0 : Vs));
 }
 
-template <typename R, int BY, bool PHS = false>
+template <typename R, int BY, bool PHS = false, bool XS = false>
 struct Slice {
   static_assert(BY % 2 == 0, "BY must be even");
   int L, nbx, nby, bx, by, x0, y0, bxl, bxr, byu, byd;
+  int lane_l, lane_r;  // XS: lanes holding the left / right neighbour tiles
   bool on;
   Cx<R>* xb[4];  // exchange buffers (Vs complex each)
   Cx<R>* phr;    // PHS: [2 Vs] all bond phases;  else [L][nbx] x-bond phases of column x0+1
@@ -87,9 +110,22 @@ struct Slice {
     L = L_;
     nbx = L / 2;
     nby = L / BY;
-    on = tid < nbx * nby;
-    bx = on ? tid % nbx : 0;
-    by = on ? tid / nbx : 0;
+    if (XS) {
+      int W = 1;
+      while (W < nbx) W <<= 1;
+      const int lane = tid & 31, seg = lane / W;
+      const int tbx = lane % W, tby = (tid >> 5) * (32 / W) + seg;
+      on = tbx < nbx && tby < nby;
+      bx = on ? tbx : 0;
+      by = on ? tby : 0;
+      lane_l = on ? seg * W + (tbx == 0 ? nbx - 1 : tbx - 1) : lane;
+      lane_r = on ? seg * W + (tbx + 1 == nbx ? 0 : tbx + 1) : lane;
+    } else {
+      on = tid < nbx * nby;
+      bx = on ? tid % nbx : 0;
+      by = on ? tid / nbx : 0;
+      lane_l = lane_r = 0;
+    }
     x0 = 2 * bx;
     y0 = BY * by;
     bxl = (bx + nbx - 1) % nbx;
@@ -143,6 +179,49 @@ struct Slice {
   // ---- bond phases of one slice --------------------------------------------
   // ang: the slice's 2*Vs angles (A = float or double); t1 = tanh(dtau),
   // th = tanh(dtau/2).  Contains one __syncthreads().
+  // angles of the owned sites of one slice (issued early to hide latency)
+  template <typename A>
+  __device__ __forceinline__ void load_angles(A (&a)[BY][4], const A* ang) const {
+    if (!on) return;
+#pragma unroll
+    for (int r = 0; r < BY; ++r) ld4(ang + 2 * ((y0 + r) * L + x0), a[r]);
+  }
+
+  // phases of a slice from angles loaded earlier by load_angles (register
+  // mode only); contains one __syncthreads().
+  template <typename A>
+  __device__ void phases_from(const A (&a)[BY][4], R t1, R th) {
+    static_assert(!PHS, "phases_from is for the register-phase engine");
+    if (on) {
+#pragma unroll
+      for (int r = 0; r < BY; ++r) {
+        tpx_[PHS ? 0 : r][0] = tphase((R)a[r][0], (r & 1) == 0 ? t1 : th);
+        tpy_[PHS ? 0 : r][0] = tphase((R)a[r][1], th);
+        tpx_[PHS ? 0 : r][1] = tphase((R)a[r][2], (r & 1) == 1 ? t1 : th);
+        tpy_[PHS ? 0 : r][1] = tphase((R)a[r][3], th);
+      }
+      if (!XS) {
+#pragma unroll
+        for (int r = 0; r < BY; ++r) phr[(y0 + r) * nbx + bx] = tpx_[PHS ? 0 : r][1];
+      }
+      phb[by * L + x0] = tpy_[PHS ? 0 : BY - 1][0];
+      phb[by * L + x0 + 1] = tpy_[PHS ? 0 : BY - 1][1];
+    }
+    if (XS) {
+#pragma unroll
+      for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = shfl_c(tpx_[PHS ? 0 : r][1], lane_l);
+    }
+    __syncthreads();
+    if (on) {
+      if (!XS) {
+#pragma unroll
+        for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = phr[(y0 + r) * nbx + bxl];
+      }
+      tpt_[0] = phb[byu * L + x0];
+      tpt_[1] = phb[byu * L + x0 + 1];
+    }
+  }
+
   template <typename A>
   __device__ void phases(const A* ang, R t1, R th) {
     if (PHS) {
@@ -173,18 +252,30 @@ struct Slice {
         tpx_[PHS ? 0 : r][1] = tphase((R)a[2], (r & 1) == 1 ? t1 : th);
         tpy_[PHS ? 0 : r][1] = tphase((R)a[3], th);
       }
+      if (!XS) {
 #pragma unroll
-      for (int r = 0; r < BY; ++r) phr[(y0 + r) * nbx + bx] = tpx_[PHS ? 0 : r][1];
+        for (int r = 0; r < BY; ++r) phr[(y0 + r) * nbx + bx] = tpx_[PHS ? 0 : r][1];
+      }
       phb[by * L + x0] = tpy_[PHS ? 0 : BY - 1][0];
       phb[by * L + x0 + 1] = tpy_[PHS ? 0 : BY - 1][1];
     }
+    if (XS) {
+#pragma unroll
+      for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = shfl_c(tpx_[PHS ? 0 : r][1], lane_l);
+    }
     __syncthreads();
     if (on) {
+      if (!XS) {
 #pragma unroll
-      for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = phr[(y0 + r) * nbx + bxl];
+        for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = phr[(y0 + r) * nbx + bxl];
+      }
       tpt_[0] = phb[byu * L + x0];
       tpt_[1] = phb[byu * L + x0 + 1];
     }
+  }
+
+  __device__ static __forceinline__ Cx<R> shfl_c(Cx<R> v, int src) {
+    return mk<R>(__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src));
   }
 
   // ---- one factor ----------------------------------------------------------
@@ -207,7 +298,33 @@ struct Slice {
   template <int G, int MODE>
   __device__ __forceinline__ void factor(Cx<R> (&v)[BY][2]) {
     const R c = (G == 0) ? c1 : ch;
-    Cx<R>* buf = xb[cur];
+    Cx<R>* buf = cur ? xb[1] : xb[0];
+    if (XS && (G == 0 || G == 2)) {
+      // neighbours' old values by shuffle; every lane takes part
+#pragma unroll
+      for (int r = 0; r < BY; ++r) {
+        if (!xcross(G, r)) {
+          if (on) pair_update<MODE>(v[r][0], v[r][1], TPX(r, 0), c);
+        } else {
+          const Cx<R> right = shfl_c(v[r][0], lane_r);
+          const Cx<R> left = shfl_c(v[r][1], lane_l);
+          if (on) {
+            Cx<R> ao = TPX(r, 1), al = TPL(r);
+            if (MODE == FAC_INV) {
+              ao = cneg(ao);
+              al = cneg(al);
+            }
+            v[r][1] = cfma(ao, right, v[r][1]);
+            v[r][0] = cjfma(al, left, v[r][0]);
+            if (MODE != FAC_TILDE) {
+              v[r][1] = c * v[r][1];
+              v[r][0] = c * v[r][0];
+            }
+          }
+        }
+      }
+      return;  // no shared-memory buffer used
+    }
     if (G == 0 || G == 2) {
       Cx<R>* xl = buf;
       Cx<R>* xr = buf + L * nbx;

@@ -61,7 +61,7 @@ class PcgSolver:
     def __init__(self, systems: Sequence[System], mode: str = "mixed", rtol: float = 1e-10,
                  max_iter: int = 10000, dtau: float = 0.1, use_precon: bool = True,
                  ru_interval: int = 50, ru_delta: float = 0.1, by: int = 0, slab: int = 0,
-                 chunk: int = 0, timeout_ms: float = 2000.0, device=None):
+                 chunk: int = 0, timeout_ms: float = 2000.0, profile: bool = False, device=None):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {sorted(MODES)}")
         self.systems = [s if isinstance(s, System) else System(*s) for s in systems]
@@ -70,9 +70,12 @@ class PcgSolver:
         n = len(self.systems)
         self._sys = (_lib.QedfSystem * n)(*[_lib.QedfSystem(s.Lx, s.Ltau, s.nrhs, 1 if s.shared_boson else 0)
                                             for s in self.systems])
+        # optional per-phase SM cycle counters of the solver kernel (block 0)
+        self.profile = torch.zeros(8, dtype=torch.int64, device=self.device) if profile else None
         self._opts = _lib.QedfPcgOpts(MODES[mode], int(max_iter), float(rtol), float(dtau),
                                       1 if use_precon else 0, int(ru_interval), float(ru_delta), int(by),
-                                      int(slab), int(chunk), float(timeout_ms))
+                                      int(slab), int(chunk), float(timeout_ms),
+                                      self.profile.data_ptr() if profile else None)
         nbytes = _lib.load().qedf_pcg_workspace_bytes(self._sys, n, self._opts)
         if nbytes < 0:
             raise ValueError("invalid system description for the PCG solver")
@@ -103,6 +106,16 @@ class PcgSolver:
                   ptr(out.iters), ptr(out.relres), ptr(out.status), ptr(self.workspace),
                   self.workspace.numel(), self._opts, stream_handle())
         return out
+
+
+    PHASES = ("init", "operator", "wait_after_operator", "elementwise", "wait_after_elementwise",
+              "reliable_updates", "bookkeeping", "total")
+
+    def phase_cycles(self) -> dict:
+        """Accumulated SM cycles per phase (needs ``profile=True``); syncs the device."""
+        if self.profile is None:
+            raise RuntimeError("construct the solver with profile=True")
+        return dict(zip(self.PHASES, self.profile.cpu().tolist()))
 
 
 def solve_pcg_batched(systems, boson, b, **kw) -> SolveResult:

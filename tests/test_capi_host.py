@@ -57,11 +57,11 @@ def test_host_validation_rejects_before_launch():
 
 def test_pcg_workspace_query():
     sys_ = (_lib.QedfSystem * 2)(_lib.QedfSystem(12, 120, 4, 0), _lib.QedfSystem(18, 180, 4, 1))
-    opts = _lib.QedfPcgOpts(_lib.QEDF_PCG_MIXED, 100, 1e-10, 0.1, 1, 50, 0.1, 0, 0, 0, 0.0)
+    opts = _lib.QedfPcgOpts(_lib.QEDF_PCG_MIXED, 100, 1e-10, 0.1, 1, 50, 0.1, 0, 0, 0, 0.0, None)
     nb = _lib.load().qedf_pcg_workspace_bytes(sys_, 2, opts)
     nvec = 4 * 12 * 12 * 120 + 4 * 18 * 18 * 180
     assert nb >= 6 * nvec * 8
-    bad = _lib.QedfPcgOpts(7, 100, 1e-10, 0.1, 1, 50, 0.1, 0, 0, 0, 0.0)
+    bad = _lib.QedfPcgOpts(7, 100, 1e-10, 0.1, 1, 50, 0.1, 0, 0, 0, 0.0, None)
     assert _lib.load().qedf_pcg_workspace_bytes(sys_, 2, bad) < 0
 
 
