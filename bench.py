@@ -53,6 +53,10 @@ def parse_args(argv=None):
     ap.add_argument("--cg-iters-per-solve", type=float, default=None,
                     help="reference arm: PCG iterations per solve used to extrapolate a trajectory")
     ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--solve-only", type=int, default=0,
+                    help="profiling mode: one PCG solve of the workload with exactly this many iterations")
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "fp32", "fp64"],
+                    help="precision of the --solve-only solve")
     ap.add_argument("--quick", action="store_true",
                     help="timed trajectories only (no e2e, FP64, Delta H, matvec or CPU legs): for profiling")
     return ap.parse_args(argv)
@@ -216,6 +220,26 @@ def pi_flux_np(rng, L, Ltau, bs):
 
 
 # ---------------------------------------------------------------------------
+# replicas: whole-job aggregation over ranks
+# ---------------------------------------------------------------------------
+def replica_seed(base_seed, rank):
+    """Independent chains per rank: a distinct seed per replica."""
+    return base_seed + 1000 * rank
+
+
+def aggregate_over_ranks(elapsed_s, trajectories_per_rank, world, dist=None, device=None):
+    """Max of the per-rank timed region over ranks (the job ends with the
+    slowest replica) and the whole-job throughput: all ranks' trajectories
+    divided by that time.  Returns (max_elapsed_s, trajectories_per_hour)."""
+    if world > 1:
+        import torch
+        t = torch.tensor([float(elapsed_s)], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_s = float(t)
+    return elapsed_s, 3600.0 * trajectories_per_rank * world / elapsed_s
+
+
+# ---------------------------------------------------------------------------
 # native arm
 # ---------------------------------------------------------------------------
 def run_native(args):
@@ -236,13 +260,13 @@ def run_native(args):
     from qed_fermion_b200.hmc import HmcSampler, ref_to_kernel
     build.build()
     L, Lt, bs = args.L, args.Ltau, args.bs
-    seed = args.seed + 1000 * rank
+    seed = replica_seed(args.seed, rank)
     rng = np.random.default_rng(seed)
 
-    def make(precision):
+    def make(precision, solver_impl="persistent"):
         h = HmcSampler(Lx=L, Ltau=Lt, J=1.0, K=1.0, dtau=0.1, bs=bs, delta_t=args.delta_t,
                        N_leapfrog=args.n_leapfrog, precision=precision, cg_rtol=args.rtol, max_iter=20000,
-                       device=dev, seed=seed)
+                       device=dev, seed=seed, solver_impl=solver_impl)
         return h
 
     hmc = make("mixed")
@@ -294,12 +318,9 @@ def run_native(args):
         torch.cuda.synchronize()
     launches = _lib.LAUNCHES["count"] - launches0
     elapsed = t_start.elapsed_time(t_end) / 1e3
+    elapsed, value = aggregate_over_ranks(elapsed, args.steps * bs, world, dist, dev)
     if world > 1:
-        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t)
         dist.barrier()
-    value = 3600.0 * args.steps * bs * world / elapsed
     clocks = clk.summary()
     acc_rate = float(torch.stack(accepted).double().mean())
 
@@ -368,7 +389,23 @@ def run_native(args):
         torch.cuda.synchronize()
         t64 = e0.elapsed_time(e1) / 1e3
         fp64 = {"value": 3600.0 * args.fp64_steps * bs / t64, "unit": UNIT, "steps": args.fp64_steps,
-                "s_per_trajectory": t64 / args.fp64_steps}
+                "s_per_trajectory": t64 / args.fp64_steps,
+                "path": "same engine in double (persistent PCG, double force)"}
+        # the drop-in path: the reference's per-iteration PCG loop on this library's
+        # _C kernels in complex128 (one trajectory, same workload)
+        hd = make("fp64", solver_impl="reference_loop")
+        hd.boson = hmc.boson.to(torch.float64)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        hd.metropolis_update()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        td = e0.elapsed_time(e1) / 1e3
+        fp64["dropin"] = {"value": 3600.0 * bs / td, "unit": UNIT, "steps": 1, "s_per_trajectory": td,
+                          "path": "reference loop structure (preconditioned_cg_fast_test) on _C kernels, "
+                                  "complex128"}
 
     # --- Delta H of one shared trajectory, mixed vs FP64
     dH = None
@@ -436,7 +473,8 @@ def run_native(args):
                          "traffic": None,
                          "bytes_model": "per PCG iteration per rhs: N*(7*8 + 2*4) B (read p,x,r,angles; write x,r,p)"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
-            "fp64_plain": fp64, "speedup_vs_fp64": (value / bs / world * bs) / fp64["value"] if fp64 else None,
+            "fp64_plain": fp64, "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
+            "speedup_vs_fp64_dropin": (value / world) / fp64["dropin"]["value"] if fp64 else None,
             "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate, **result,
         }
         print(json.dumps(line), flush=True)
@@ -446,10 +484,46 @@ def run_native(args):
     return 0
 
 
+def run_solve_only(args):
+    """One PCG solve on the bench workload with a fixed iteration count (rtol 0):
+    the small, self-contained launch that ncu captures of the solver use."""
+    import numpy as np
+    import torch
+    from qed_fermion_b200 import build
+    from qed_fermion_b200.hmc import ref_to_kernel
+    from qed_fermion_b200.solver import PcgSolver, System
+    build.build()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(args.seed)
+    L, Lt, bs = args.L, args.Ltau, args.bs
+    phi = ref_to_kernel(torch.tensor(pi_flux_np(rng, L, Lt, bs), device=dev))
+    b = torch.randn((bs, L * L * Lt), dtype=torch.complex128, device=dev,
+                    generator=torch.Generator(device=dev).manual_seed(args.seed)) / math.sqrt(2)
+    s = PcgSolver([System(L, Lt, bs)], mode=args.mode, rtol=0.0, max_iter=args.solve_only, device=dev)
+    args_ = (phi.to(s.angle_dtype), b.to(s.vec_dtype))
+    s.solve(*args_)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res = s.solve(*args_)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    it = int(res.iters.max())
+    n = L * L * Lt * bs
+    print(json.dumps({"solve_only": True, "mode": args.mode, "lattice": [L, L, Lt], "rhs": bs, "iters": it,
+                      "ms": ms, "us_per_iter": ms * 1e3 / max(it, 1),
+                      "algorithmic_GBps": n * 64 * it / (ms / 1e3) / 1e9}), flush=True)
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.solve_only > 0:
+        return run_solve_only(args)
     return run_native(args)
 
 

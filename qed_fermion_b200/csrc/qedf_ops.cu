@@ -26,7 +26,7 @@ namespace qedf {
 //                  applied to it, so x is read once and one extra slice of y
 //                  (the slab's lower halo) is recomputed.
 template <typename R, typename A, int BY, int OP, int EC>
-__global__ void __launch_bounds__(MaxT<BY, EC>::value, 1) k_operator(OpArgs p) {
+__global__ void __launch_bounds__(MaxT<BY, EC>::value, MaxT<BY, EC>::min_blocks) k_operator(OpArgs p) {
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr bool PHS = (EC & EC_PHS) != 0;
   constexpr bool STASH = (EC & EC_NOSTASH) == 0;
@@ -590,6 +590,8 @@ template <typename R, typename A, int BY>
 static int launch_operator_by(int op, const OpArgs& a, int xs, cudaStream_t st) {
   if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
     return launch_operator_t<R, A, BY, EC_PHS>(op, a, st);
+  if (sizeof(R) == 4 && a.variant == 1 && 2 * slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
+    return launch_operator_t<R, A, BY, EC_PHS | EC_2CTA>(op, a, st);
   if (sizeof(R) == 4 && xs && xs_possible(a.L) && ((a.L / 2) & (a.L / 2 - 1)) == 0 &&
       slice_threads(a.L, BY, true) <= MaxT<BY, EC_XS>::value)
     return launch_operator_t<R, A, BY, EC_XS>(op, a, st);

@@ -48,7 +48,8 @@ struct MaxThreads {
 //   EC_XS      exchanges of the x-bond factors by warp shuffles: a warp holds
 //              whole rows of tiles (L/2 <= 32 tiles per row, padded to a power
 //              of two), so only the y-bond factors need a block barrier
-enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4 };
+//   EC_2CTA    compiled for two resident blocks per SM (register budget halved)
+enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_2CTA = 8 };
 
 // Largest thread block of a kernel compiled for tile height BY and engine
 // configuration EC (it fixes the register budget: 65536 / value per thread).
@@ -56,6 +57,7 @@ template <int BY, int EC>
 struct MaxT {
   static constexpr int value = (EC & EC_XS) ? (BY == 2 ? 768 : (BY == 4 ? 512 : 384))
                                             : (BY == 2 ? 576 : (BY == 4 ? 512 : 384));
+  static constexpr int min_blocks = (EC & EC_2CTA) ? 2 : 1;
 };
 
 // threads of one slice engine (a multiple of 32)

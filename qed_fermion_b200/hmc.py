@@ -42,7 +42,7 @@ def kernel_to_ref(phi: torch.Tensor, Lx: int, Ltau: int) -> torch.Tensor:
 class HmcSampler:
     def __init__(self, Lx=6, Ltau=10, J=1.0, K=1.0, dtau=0.1, bs=1, delta_t=0.06, N_leapfrog=5, m=1.0,
                  compact=False, precision="mixed", cg_rtol=1e-10, max_iter=20000, use_precon=True,
-                 ru_interval=50, ru_delta=0.1, device=None, seed=None):
+                 ru_interval=50, ru_delta=0.1, device=None, seed=None, solver_impl="persistent"):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}")
         if Lx % 2:
@@ -75,6 +75,13 @@ class HmcSampler:
         self.solver = PcgSolver([System(Lx, Ltau, bs, False)], mode=solver_mode, rtol=cg_rtol, max_iter=max_iter,
                                 dtau=dtau, use_precon=self.use_precon, ru_interval=ru_interval,
                                 ru_delta=ru_delta, device=self.device)
+        # "persistent": one cooperative PCG kernel per solve; "reference_loop": the
+        # reference's per-iteration launch sequence (preconditioned_cg_fast_test) on
+        # this library's _C kernels -- the drop-in path
+        if solver_impl not in ("persistent", "reference_loop"):
+            raise ValueError("solver_impl must be 'persistent' or 'reference_loop'")
+        self.solver_impl = solver_impl
+        self._precon_tau = None
         self.boson = None
         self.last_cg_iters = None
 
@@ -138,6 +145,15 @@ class HmcSampler:
     def Ot_inv_psi_fast(self, psi, boson_k, MhM=None):
         """xi = (M^dag M)^{-1} psi with the persistent batched PCG.
         ``boson_k``: kernel-layout angles ``[bs, ...]``; returns (xi, iters, relres)."""
+        if self.solver_impl == "reference_loop":
+            if self._precon_tau is None and self.use_precon:
+                from . import precon
+                self._precon_tau = precon.to_device(precon.builtin_tau_csr(self.Ltau), self.device)
+            adt = torch.float64 if self.cdtype == torch.complex128 else torch.float32
+            x, it, err = self.preconditioned_cg_fast_test(boson_k.to(adt), psi.to(self.cdtype),
+                                                          precon_tau=self._precon_tau)
+            self.last_cg_iters = it
+            return x.view(self.bs, -1), it, err
         res = self.solver.solve(self._angles_for_solver(boson_k), psi.to(self.solver.vec_dtype))
         self.last_cg_iters = res.iters
         self.last_status = res.status
