@@ -200,6 +200,25 @@ int qedf_pcg_solve(const qedf_system* sys, int nsys, const void* boson, const vo
                    int* iters, double* relres, int* status, void* workspace, int64_t workspace_bytes,
                    const qedf_pcg_opts* opts, qedf_stream_t stream);
 
+/* ---------------------------------------------------------------------------
+ * Allocation-free solve.  No counterpart in the reference: it exists for hosts
+ * that cannot allocate device memory where they solve (a driver capturing a
+ * CUDA graph, or running under an allocator or a fixed memory budget it does
+ * not control).  Same inputs, outputs and status as qedf_pcg_solve, but the
+ * workspace is a device array inside this library of
+ * QEDF_PCG_STATIC_SCRATCH_BYTES bytes per GPU, held by every GPU that loads the
+ * library until exit.  Problems whose qedf_pcg_workspace_bytes exceeds it get
+ * QEDF_ERR_SIZE.  Calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller.  The first call on a device looks up the
+ * array's device address (once per device, that device current); make it
+ * before any stream capture begins.  It calls no cudaMalloc or other allocator.
+ * ------------------------------------------------------------------------- */
+#define QEDF_PCG_STATIC_SCRATCH_BYTES (64ll << 20)
+
+int qedf_pcg_solve_static(const qedf_system* sys, int nsys, const void* boson, const void* b, void* x,
+                          int* iters, double* relres, int* status, const qedf_pcg_opts* opts,
+                          qedf_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

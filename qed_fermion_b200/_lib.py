@@ -72,6 +72,10 @@ SIGNATURES["qedf_precon_tau_csr"] = (c_int, [c_int, POINTER(c_int), POINTER(c_in
 SIGNATURES["qedf_pcg_workspace_bytes"] = (c_int64, [POINTER(QedfSystem), c_int, POINTER(QedfPcgOpts)])
 SIGNATURES["qedf_pcg_solve"] = (c_int, [POINTER(QedfSystem), c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, c_int64,
                                         POINTER(QedfPcgOpts), _vp])
+SIGNATURES["qedf_pcg_solve_static"] = (c_int, [POINTER(QedfSystem), c_int, _vp, _vp, _vp, _vp, _vp, _vp,
+                                               POINTER(QedfPcgOpts), _vp])
+# bytes of the library's own device scratch used by qedf_pcg_solve_static
+PCG_STATIC_SCRATCH_BYTES = 64 << 20
 
 _LIB = None
 # kernel launches issued through ``call`` (compute entry points launch one
@@ -111,7 +115,7 @@ def call(name, *args):
     st = getattr(lib, name)(*args)
     if name not in _HOST_ONLY:
         # qedf_pcg_solve launches a small preparation kernel and the solver
-        LAUNCHES["count"] += 2 if name == "qedf_pcg_solve" else 1
+        LAUNCHES["count"] += 2 if name.startswith("qedf_pcg_solve") else 1
     if st != QEDF_OK:
         raise QedfError(name, st, lib.qedf_status_string(st).decode())
     return st

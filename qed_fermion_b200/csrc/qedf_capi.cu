@@ -168,6 +168,63 @@ int kick_entry(A* p, const A* F, A* x, const double* dt, const float* mask, doub
 
 }  // namespace
 
+namespace qedf {
+
+// Solve with a caller-provided workspace (shared by qedf_pcg_solve and the
+// static-scratch entry point).
+int pcg_solve_ws(const qedf_system* sys, int nsys, const void* boson, const void* b, void* x, int* iters,
+                 double* relres, int* status, void* workspace, int64_t ws_bytes, const qedf_pcg_opts* opts,
+                 qedf_stream_t stream) {
+  PcgParams p;
+  int e = pcg_plan(p, sys, nsys, opts);
+  if (e) return e;
+  p.variant = std::getenv("QEDF_VARIANT") ? std::atoi(std::getenv("QEDF_VARIANT")) : 0;
+  if (!boson || !b || !x || !iters || !relres || !status || !workspace) return QEDF_ERR_ARG;
+  if (!aligned16(boson) || !aligned16(b) || !aligned16(x) || !aligned16(workspace)) return QEDF_ERR_ARG;
+  if (opts->max_iter < 0 || !(opts->rtol >= 0)) return QEDF_ERR_ARG;
+  const int sb = opts->mode == QEDF_PCG_PLAIN_F64 ? 8 : 4;
+  const size_t need = pcg_workspace_bytes(p, sb);
+  if (ws_bytes < (int64_t)need) return QEDF_ERR_ARG;
+  // carve the workspace
+  unsigned char* w = reinterpret_cast<unsigned char*>(workspace);
+  const size_t vecb = ((size_t)p.nvec_total * 2 * sb + 255) / 256 * 256;
+  p.r = w;
+  p.p0 = w + vecb;
+  p.p1 = w + 2 * vecb;
+  p.z = w + 3 * vecb;
+  p.Op = w + 4 * vecb;
+  size_t off = 5 * vecb;
+  if (p.mode == QEDF_PCG_MIXED) {
+    p.xlo = w + off;
+    off += vecb;
+  }
+  p.acc = reinterpret_cast<double*>(w + off);
+  const size_t accb = ((sizeof(double) * 9 * p.nrhs) + 255) / 256 * 256;
+  off += accb;
+  p.bar = reinterpret_cast<unsigned int*>(w + off);
+  off += 256;
+  p.ptab = reinterpret_cast<float*>(w + off);
+  p.phi = boson;
+  p.b = b;
+  p.x = x;
+  p.iters = iters;
+  p.relres = relres;
+  p.status = status;
+  p.prof = opts->profile;
+  const double tmo = opts->timeout_ms > 0 ? opts->timeout_ms : 2000.0;
+  int dev = 0, clk_khz = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, dev);
+  if (clk_khz <= 0) clk_khz = 2000000;
+  p.timeout_cycles = (long long)(tmo * (double)clk_khz);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // accumulators and barrier state start at zero; preconditioner tables
+  if (int e2 = launch_pcg_prep(p, (int)((accb + 256) / 4), st)) return e2;
+  return launch_pcg(p, opts->by, st);
+}
+
+}  // namespace qedf
+
 extern "C" {
 
 const char* qedf_version(void) { return "qedf 0.1.0 (sm_100a)"; }
@@ -281,52 +338,7 @@ int64_t qedf_pcg_workspace_bytes(const qedf_system* sys, int nsys, const qedf_pc
 int qedf_pcg_solve(const qedf_system* sys, int nsys, const void* boson, const void* b, void* x, int* iters,
                    double* relres, int* status, void* workspace, int64_t ws_bytes, const qedf_pcg_opts* opts,
                    qedf_stream_t stream) {
-  PcgParams p;
-  int e = pcg_plan(p, sys, nsys, opts);
-  if (e) return e;
-  p.variant = std::getenv("QEDF_VARIANT") ? std::atoi(std::getenv("QEDF_VARIANT")) : 0;
-  if (!boson || !b || !x || !iters || !relres || !status || !workspace) return QEDF_ERR_ARG;
-  if (!aligned16(boson) || !aligned16(b) || !aligned16(x) || !aligned16(workspace)) return QEDF_ERR_ARG;
-  if (opts->max_iter < 0 || !(opts->rtol >= 0)) return QEDF_ERR_ARG;
-  const int sb = opts->mode == QEDF_PCG_PLAIN_F64 ? 8 : 4;
-  const size_t need = pcg_workspace_bytes(p, sb);
-  if (ws_bytes < (int64_t)need) return QEDF_ERR_ARG;
-  // carve the workspace
-  unsigned char* w = reinterpret_cast<unsigned char*>(workspace);
-  const size_t vecb = ((size_t)p.nvec_total * 2 * sb + 255) / 256 * 256;
-  p.r = w;
-  p.p0 = w + vecb;
-  p.p1 = w + 2 * vecb;
-  p.z = w + 3 * vecb;
-  p.Op = w + 4 * vecb;
-  size_t off = 5 * vecb;
-  if (p.mode == QEDF_PCG_MIXED) {
-    p.xlo = w + off;
-    off += vecb;
-  }
-  p.acc = reinterpret_cast<double*>(w + off);
-  const size_t accb = ((sizeof(double) * 9 * p.nrhs) + 255) / 256 * 256;
-  off += accb;
-  p.bar = reinterpret_cast<unsigned int*>(w + off);
-  off += 256;
-  p.ptab = reinterpret_cast<float*>(w + off);
-  p.phi = boson;
-  p.b = b;
-  p.x = x;
-  p.iters = iters;
-  p.relres = relres;
-  p.status = status;
-  p.prof = opts->profile;
-  const double tmo = opts->timeout_ms > 0 ? opts->timeout_ms : 2000.0;
-  int dev = 0, clk_khz = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, dev);
-  if (clk_khz <= 0) clk_khz = 2000000;
-  p.timeout_cycles = (long long)(tmo * (double)clk_khz);
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  // accumulators and barrier state start at zero; preconditioner tables
-  if (int e2 = launch_pcg_prep(p, (int)((accb + 256) / 4), st)) return e2;
-  return launch_pcg(p, opts->by, st);
+  return qedf::pcg_solve_ws(sys, nsys, boson, b, x, iters, relres, status, workspace, ws_bytes, opts, stream);
 }
 
 }  // extern "C"

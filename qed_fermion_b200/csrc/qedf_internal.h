@@ -140,5 +140,8 @@ size_t pcg_workspace_bytes(const PcgParams& p, int sloppy_bytes);
 int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts* o);
 int launch_pcg(PcgParams& p, int by, cudaStream_t st);
 int launch_pcg_prep(const PcgParams& p, int zero_words, cudaStream_t st);
+int pcg_solve_ws(const qedf_system* sys, int nsys, const void* boson, const void* b, void* x, int* iters,
+                 double* relres, int* status, void* workspace, int64_t ws_bytes, const qedf_pcg_opts* opts,
+                 qedf_stream_t stream);
 
 }  // namespace qedf
