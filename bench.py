@@ -55,8 +55,10 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--solve-only", type=int, default=0,
                     help="profiling mode: one PCG solve of the workload with exactly this many iterations")
+    ap.add_argument("--matvec-only", type=int, default=0,
+                    help="only time M^dag M on this many right-hand sides (c64; c128 with --mode fp64)")
     ap.add_argument("--mode", default="mixed", choices=["mixed", "fp32", "fp64"],
-                    help="precision of the --solve-only solve")
+                    help="precision of the --solve-only solve or --matvec-only launch")
     ap.add_argument("--quick", action="store_true",
                     help="timed trajectories only (no e2e, FP64, Delta H, matvec or CPU legs): for profiling")
     return ap.parse_args(argv)
@@ -518,12 +520,46 @@ def run_solve_only(args):
     return 0
 
 
+def run_matvec_only(args):
+    """Three warm-up and ten timed launches of M^dag M on the bench lattice: the
+    small, self-contained case that ncu captures of the operator kernel use."""
+    import torch
+    from qed_fermion_b200 import build, ops
+    build.build()
+    dev = torch.device("cuda", 0)
+    L, Lt, nr = args.L, args.Ltau, args.matvec_only
+    N = L * L * Lt
+    c128 = args.mode == "fp64"
+    rdt, cdt, bps = (torch.float64, torch.complex128, 48) if c128 else (torch.float32, torch.complex64, 24)
+    g = torch.Generator(device=dev).manual_seed(args.seed)
+    phi = torch.rand((nr, 2 * N), device=dev, dtype=rdt, generator=g) * 6.28 - 3.14
+    xv = torch.randn((nr, N), device=dev, dtype=cdt, generator=g)
+    out = torch.empty_like(xv)
+    for _ in range(3):
+        ops.apply_operator("mhm", phi, xv, L, 0.1, out=out)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 10
+    e0.record()
+    for _ in range(reps):
+        ops.apply_operator("mhm", phi, xv, L, 0.1, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    print(json.dumps({"matvec_only": True, "dtype": "c128" if c128 else "c64", "lattice": [L, L, Lt], "rhs": nr,
+                      "ms_per_launch": ms, "GBps": bps * N * nr / (ms / 1e3) / 1e9}), flush=True)
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
     if args.solve_only > 0:
         return run_solve_only(args)
+    if args.matvec_only > 0:
+        return run_matvec_only(args)
     return run_native(args)
 
 
