@@ -12,8 +12,10 @@
 
 namespace qedf {
 
+// 8-byte (complex64) / 16-byte (complex128) alignment, so that one complex
+// moves with one vector access
 template <typename R>
-struct Cx {
+struct alignas(2 * sizeof(R)) Cx {
   R re, im;
 };
 

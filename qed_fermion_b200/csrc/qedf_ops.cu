@@ -213,18 +213,16 @@ struct ForceSlice {
     const R c = (G == 0) ? S.c1 : S.ch;
     Cx<R>* bR = S.xb[2 * par];
     Cx<R>* bl = S.xb[2 * par + 1];
-    const int L = S.L, nbx = S.nbx, nby = S.nby;
     if (G == 0 || G == 2) {
-      const int half = L * nbx;
+      // cross row r uses slots r & ~1 (left column) and (r & ~1) + 1 (right column)
       if (S.on) {
 #pragma unroll
         for (int r = 0; r < BY; ++r)
           if (Slice<R, BY, PHS>::xcross(G, r)) {
-            const int q = (S.y0 + r) * nbx + S.bx;
-            bR[q] = Rv[r][0];
-            bR[half + q] = Rv[r][1];
-            bl[q] = l[r][0];
-            bl[half + q] = l[r][1];
+            S.slot(bR, r & ~1)[S.id] = Rv[r][0];
+            S.slot(bR, (r & ~1) + 1)[S.id] = Rv[r][1];
+            S.slot(bl, r & ~1)[S.id] = l[r][0];
+            S.slot(bl, (r & ~1) + 1)[S.id] = l[r][1];
           }
       }
       __syncthreads();
@@ -243,9 +241,8 @@ struct ForceSlice {
           Rv[r][0] = nRi;
           Rv[r][1] = nRj;
         } else {
-          const int q = (S.y0 + r) * nbx;
-          const Cx<R> Rright = bR[q + S.bxr], lright = bl[q + S.bxr];
-          const Cx<R> Rleft = bR[half + q + S.bxl], lleft = bl[half + q + S.bxl];
+          const Cx<R> Rright = S.slot(bR, r & ~1)[S.idr], lright = S.slot(bl, r & ~1)[S.idr];
+          const Cx<R> Rleft = S.slot(bR, (r & ~1) + 1)[S.idl], lleft = S.slot(bl, (r & ~1) + 1)[S.idl];
           // pair (i = own x0+1, j = right neighbour's x0), phase own
           const Cx<R> a = S.TPX(r, 1);
           const Cx<R> nRi = c * cfma(cneg(a), Rright, Rv[r][1]);
@@ -265,13 +262,11 @@ struct ForceSlice {
     } else {
       constexpr int CL = (G == 1) ? 0 : 1;
       constexpr int CC = 1 - CL;
-      const int half = nby * L;
       if (S.on) {
-        const int q = S.by * L + S.x0 + CC;
-        bR[q] = Rv[0][CC];
-        bR[half + q] = Rv[BY - 1][CC];
-        bl[q] = l[0][CC];
-        bl[half + q] = l[BY - 1][CC];
+        S.slot(bR, 0)[S.id] = Rv[0][CC];
+        S.slot(bR, 1)[S.id] = Rv[BY - 1][CC];
+        S.slot(bl, 0)[S.id] = l[0][CC];
+        S.slot(bl, 1)[S.id] = l[BY - 1][CC];
       }
       __syncthreads();
       if (!S.on) return;
@@ -303,10 +298,8 @@ struct ForceSlice {
         Rv[r + 1][CC] = nRj;
       }
       // bottom pair: i = own last row, j = lower neighbour's first row
-      const int qd = S.byd * L + S.x0 + CC;
-      const int qu = S.byu * L + S.x0 + CC;
-      const Cx<R> Rbelow = bR[qd], lbelow = bl[qd];
-      const Cx<R> Rabove = bR[half + qu], labove = bl[half + qu];
+      const Cx<R> Rbelow = S.slot(bR, 0)[S.idd], lbelow = S.slot(bl, 0)[S.idd];
+      const Cx<R> Rabove = S.slot(bR, 1)[S.idu], labove = S.slot(bl, 1)[S.idu];
       const Cx<R> ab = S.TPY(BY - 1, CC);
       const Cx<R> at = S.TPT(CC);
       const Cx<R> Rb = Rv[BY - 1][CC], lb = l[BY - 1][CC];

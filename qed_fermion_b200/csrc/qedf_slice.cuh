@@ -1,10 +1,11 @@
 // Slice engine: applies the checkerboard bond factors of one imaginary-time
 // slice to a vector held in registers by one thread block.
 //
-// Thread mapping.  The L x L slice is tiled by 2 x BY site blocks; thread
-// (bx, by) owns x in {2bx, 2bx+1} and y in [BY*by, BY*by + BY).  Because x0
-// and y0 are even, every bond factor pairs sites either inside the block
-// ("local") or across its edge with the neighbouring block ("cross"):
+// Thread mapping.  The L x L slice is tiled by 2 x BY site blocks ("tiles");
+// tile (bx, by) owns x in {2bx, 2bx+1} and y in [BY*by, BY*by + BY) and has
+// the id by * nbx + bx (its thread index, except in the shuffle variant).
+// Because x0 and y0 are even, every bond factor pairs sites either inside the
+// tile ("local") or across its edge with the neighbouring tile ("cross"):
 //
 //   g1 (x-bond A -> A+x):  local in even rows, cross in odd rows
 //   g3 (x-bond A-x -> A):  local in odd rows,  cross in even rows
@@ -20,6 +21,10 @@
 // once by the owner of the bond's origin site and kept in registers; the
 // phases a thread needs from its left and upper neighbours go through shared
 // memory once per slice.
+//
+// Shared-memory layout.  Every table is indexed [slot][tile id], so the lanes
+// of a warp touch consecutive words (no bank conflicts apart from the wrap at
+// the ends of a tile row), and a neighbour's value sits at the neighbour's id.
 #pragma once
 
 #include "qedf_common.cuh"
@@ -35,16 +40,11 @@ struct MaxThreads {
   static constexpr int value = BY == 2 ? 576 : (BY == 4 ? 512 : 384);
 };
 
-// Shared-memory size (bytes) of one slice engine: nbuf exchange buffers, the
-// phase tables and a thread-private stash of one vector.  PHS = false keeps a
-// thread's own bond phases in registers and only the neighbours' in shared
-// memory; PHS = true (used in double precision to relieve registers) keeps
-// the phases of all 2 Vs bonds of the slice in shared memory.
-//
 // Engine configuration bits (template parameter EC of the kernels):
 //   EC_PHS     phases of all bonds in shared memory (else own ones in registers)
 //   EC_NOSTASH no shared-memory stash: the previous y block stays in registers
-// (used only where the shared memory of the default layout does not fit).
+//              (used only where the shared memory of the default layout does
+//              not fit)
 //   EC_XS      exchanges of the x-bond factors by warp shuffles: a warp holds
 //              whole rows of tiles (L/2 <= 32 tiles per row, padded to a power
 //              of two), so only the y-bond factors need a block barrier
@@ -71,47 +71,59 @@ __host__ __device__ inline int slice_threads(int L, int BY, bool xs) {
 }
 __host__ __device__ inline bool xs_possible(int L) { return L / 2 <= 32; }
 
+// Shared-memory size (bytes) of one slice engine with NT = L^2 / (2 BY) tiles:
+//   nbuf exchange buffers of BY * NT complex (x-bond factors: a left and a
+//        right slot per cross row; y-bond factors: a top and a bottom slot),
+//   phase tables: PHS [4][BY][NT] (all bonds), else [BY + 2][NT] (the
+//        x-bond phases of column x0+1 and the y-bond phases of the last row),
+//   the thread-private stash of one vector block, [2 BY][NT] complex.
 template <typename R, int EC = 0>
 __host__ __device__ inline size_t slice_smem_bytes(int L, int BY, int nbuf) {
-  const size_t Vs = (size_t)L * L;
-  const size_t ph = (EC & EC_PHS) ? 2 * Vs : Vs / 2 + Vs / BY;
-  return sizeof(Cx<R>) * (nbuf * Vs + ph + ((EC & EC_NOSTASH) ? 0 : Vs));
+  const size_t NT = (size_t)(L / 2) * (L / BY);
+  const size_t ph = (EC & EC_PHS) ? 4 * BY * NT : (BY + 2) * NT;
+  return sizeof(Cx<R>) * (nbuf * BY * NT + ph + ((EC & EC_NOSTASH) ? 0 : 2 * BY * NT));
 }
 
 template <typename R, int BY, bool PHS = false, bool XS = false>
 struct Slice {
   static_assert(BY % 2 == 0, "BY must be even");
-  int L, nbx, nby, bx, by, x0, y0, bxl, bxr, byu, byd;
-  int lane_l, lane_r;  // XS: lanes holding the left / right neighbour tiles
+  int L, nbx, nby, NT, bx, by, x0, y0, bxl, bxr, byu, byd;
+  int id, idl, idr, idu, idd;  // tile ids of this tile and of its four neighbours
+  int lane_l, lane_r;          // XS: lanes holding the left / right neighbour tiles
   bool on;
-  Cx<R>* xb[4];  // exchange buffers (Vs complex each)
-  Cx<R>* phr;    // PHS: [2 Vs] all bond phases;  else [L][nbx] x-bond phases of column x0+1
-  Cx<R>* phb;    // (register mode) [nby][L] y-bond phases of the last row of every block
-  Cx<R>* stash;  // [Vs]       each thread parks its own block of one vector here
+  Cx<R>* xb[4];  // exchange buffers (BY * NT complex each)
+  Cx<R>* ph;     // phase tables (see slice_smem_bytes)
+  Cx<R>* stash;  // [2 BY][NT] each thread parks its own block of one vector here
   int cur;
   R c1, ch;      // cosh(dtau), cosh(dtau/2)
   Cx<R> tpx_[PHS ? 1 : BY][2], tpy_[PHS ? 1 : BY][2], tpl_[PHS ? 1 : BY], tpt_[2];
 
   // phase of the x-bond / y-bond starting at own site (x0+c, y0+r), of the
   // x-bond arriving from the left in row r, of the y-bond arriving from above
+  // (PHS table slots: 0 x-bond c=0, 1 y-bond c=0, 2 x-bond c=1, 3 y-bond c=1)
   __device__ __forceinline__ Cx<R> TPX(int r, int c) const {
-    return PHS ? phr[2 * ((y0 + r) * L + x0 + c)] : tpx_[PHS ? 0 : r][c];
+    return PHS ? ph[(size_t)(2 * c * BY + r) * NT + id] : tpx_[PHS ? 0 : r][c];
   }
   __device__ __forceinline__ Cx<R> TPY(int r, int c) const {
-    return PHS ? phr[2 * ((y0 + r) * L + x0 + c) + 1] : tpy_[PHS ? 0 : r][c];
+    return PHS ? ph[(size_t)((2 * c + 1) * BY + r) * NT + id] : tpy_[PHS ? 0 : r][c];
   }
   __device__ __forceinline__ Cx<R> TPL(int r) const {
-    return PHS ? phr[2 * ((y0 + r) * L + (x0 + L - 1) % L)] : tpl_[PHS ? 0 : r];
+    return PHS ? ph[(size_t)(2 * BY + r) * NT + idl] : tpl_[PHS ? 0 : r];
   }
   __device__ __forceinline__ Cx<R> TPT(int c) const {
-    return PHS ? phr[2 * (((y0 + L - 1) % L) * L + x0 + c) + 1] : tpt_[c];
+    return PHS ? ph[(size_t)((2 * c + 1) * BY + BY - 1) * NT + idu] : tpt_[c];
   }
+  // exchange slots of a buffer: x factors use slot r & ~1 (left column) and
+  // (r & ~1) + 1 (right column) of cross row r; y factors slot 0 (top row)
+  // and slot 1 (bottom row)
+  __device__ __forceinline__ Cx<R>* slot(Cx<R>* buf, int s) const { return buf + (size_t)s * NT; }
 
-  // smem must hold slice_smem_bytes<R, PHS>(L, BY, nbuf)
+  // smem must hold slice_smem_bytes<R, EC>(L, BY, nbuf) for the kernel's EC
   __device__ void init(int L_, unsigned char* smem, int nbuf, R c1_, R ch_, int tid) {
     L = L_;
     nbx = L / 2;
     nby = L / BY;
+    NT = nbx * nby;
     if (XS) {
       int W = 1;
       while (W < nbx) W <<= 1;
@@ -123,7 +135,7 @@ struct Slice {
       lane_l = on ? seg * W + (tbx == 0 ? nbx - 1 : tbx - 1) : lane;
       lane_r = on ? seg * W + (tbx + 1 == nbx ? 0 : tbx + 1) : lane;
     } else {
-      on = tid < nbx * nby;
+      on = tid < NT;
       bx = on ? tid % nbx : 0;
       by = on ? tid / nbx : 0;
       lane_l = lane_r = 0;
@@ -134,12 +146,15 @@ struct Slice {
     bxr = (bx + 1) % nbx;
     byu = (by + nby - 1) % nby;
     byd = (by + 1) % nby;
-    const int Vs = L * L;
+    id = by * nbx + bx;
+    idl = by * nbx + bxl;
+    idr = by * nbx + bxr;
+    idu = byu * nbx + bx;
+    idd = byd * nbx + bx;
     Cx<R>* base = reinterpret_cast<Cx<R>*>(smem);
-    for (int i = 0; i < 4; ++i) xb[i] = base + (size_t)(i < nbuf ? i : 0) * Vs;
-    phr = base + (size_t)nbuf * Vs;
-    phb = phr + Vs / 2;
-    stash = PHS ? phr + 2 * Vs : phb + Vs / BY;
+    for (int i = 0; i < 4; ++i) xb[i] = base + (size_t)(i < nbuf ? i : 0) * BY * NT;
+    ph = base + (size_t)nbuf * BY * NT;
+    stash = ph + (size_t)(PHS ? 4 * BY : BY + 2) * NT;
     cur = 0;
     c1 = c1_;
     ch = ch_;
@@ -165,22 +180,22 @@ struct Slice {
     if (!on) return;
 #pragma unroll
     for (int r = 0; r < BY; ++r) {
-      stash[(y0 + r) * L + x0] = v[r][0];
-      stash[(y0 + r) * L + x0 + 1] = v[r][1];
+      slot(stash, 2 * r)[id] = v[r][0];
+      slot(stash, 2 * r + 1)[id] = v[r][1];
     }
   }
   __device__ __forceinline__ void unpark(Cx<R> (&v)[BY][2]) const {
     if (!on) return;
 #pragma unroll
     for (int r = 0; r < BY; ++r) {
-      v[r][0] = stash[(y0 + r) * L + x0];
-      v[r][1] = stash[(y0 + r) * L + x0 + 1];
+      v[r][0] = slot(stash, 2 * r)[id];
+      v[r][1] = slot(stash, 2 * r + 1)[id];
     }
   }
 
   // ---- bond phases of one slice --------------------------------------------
   // ang: the slice's 2*Vs angles (A = float or double); t1 = tanh(dtau),
-  // th = tanh(dtau/2).  Contains one __syncthreads().
+  // th = tanh(dtau/2).
   // angles of the owned sites of one slice (issued early to hide latency)
   template <typename A>
   __device__ __forceinline__ void load_angles(A (&a)[BY][4], const A* ang) const {
@@ -189,14 +204,17 @@ struct Slice {
     for (int r = 0; r < BY; ++r) ld4(ang + 2 * ((y0 + r) * L + x0), a[r]);
   }
 
-  // phases of a slice from angles loaded earlier by load_angles (register
-  // mode only); contains one __syncthreads().
+  // register mode: own phases into registers, the neighbours' through the
+  // tables; contains one __syncthreads()
   template <typename A>
   __device__ void phases_from(const A (&a)[BY][4], R t1, R th) {
     static_assert(!PHS, "phases_from is for the register-phase engine");
+    Cx<R>* phx = ph;                    // [BY][NT] x-bond phase of column x0+1
+    Cx<R>* phy = ph + (size_t)BY * NT;  // [2][NT]  y-bond phases of row y0+BY-1
     if (on) {
 #pragma unroll
       for (int r = 0; r < BY; ++r) {
+        // x-bond of (x0+c, y0+r) is in g1 when the site is an A site, else g3
         tpx_[PHS ? 0 : r][0] = tphase((R)a[r][0], (r & 1) == 0 ? t1 : th);
         tpy_[PHS ? 0 : r][0] = tphase((R)a[r][1], th);
         tpx_[PHS ? 0 : r][1] = tphase((R)a[r][2], (r & 1) == 1 ? t1 : th);
@@ -204,10 +222,10 @@ struct Slice {
       }
       if (!XS) {
 #pragma unroll
-        for (int r = 0; r < BY; ++r) phr[(y0 + r) * nbx + bx] = tpx_[PHS ? 0 : r][1];
+        for (int r = 0; r < BY; ++r) phx[(size_t)r * NT + id] = tpx_[PHS ? 0 : r][1];
       }
-      phb[by * L + x0] = tpy_[PHS ? 0 : BY - 1][0];
-      phb[by * L + x0 + 1] = tpy_[PHS ? 0 : BY - 1][1];
+      phy[id] = tpy_[PHS ? 0 : BY - 1][0];
+      phy[NT + id] = tpy_[PHS ? 0 : BY - 1][1];
     }
     if (XS) {
 #pragma unroll
@@ -217,62 +235,34 @@ struct Slice {
     if (on) {
       if (!XS) {
 #pragma unroll
-        for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = phr[(y0 + r) * nbx + bxl];
+        for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = phx[(size_t)r * NT + idl];
       }
-      tpt_[0] = phb[byu * L + x0];
-      tpt_[1] = phb[byu * L + x0 + 1];
+      tpt_[0] = phy[idu];
+      tpt_[1] = phy[NT + idu];
     }
   }
 
+  // phases of one slice straight from the angles; contains one __syncthreads()
   template <typename A>
   __device__ void phases(const A* ang, R t1, R th) {
-    if (PHS) {
+    if constexpr (PHS) {
       if (on) {
 #pragma unroll
         for (int r = 0; r < BY; ++r) {
           A a[4];
           ld4(ang + 2 * ((y0 + r) * L + x0), a);
-          Cx<R>* q = phr + 2 * ((y0 + r) * L + x0);
           // x-bond of (x0+c, y0+r) is in g1 when the site is an A site, else g3
-          q[0] = tphase((R)a[0], (r & 1) == 0 ? t1 : th);
-          q[1] = tphase((R)a[1], th);
-          q[2] = tphase((R)a[2], (r & 1) == 1 ? t1 : th);
-          q[3] = tphase((R)a[3], th);
+          ph[(size_t)(0 * BY + r) * NT + id] = tphase((R)a[0], (r & 1) == 0 ? t1 : th);
+          ph[(size_t)(1 * BY + r) * NT + id] = tphase((R)a[1], th);
+          ph[(size_t)(2 * BY + r) * NT + id] = tphase((R)a[2], (r & 1) == 1 ? t1 : th);
+          ph[(size_t)(3 * BY + r) * NT + id] = tphase((R)a[3], th);
         }
       }
       __syncthreads();
-      return;
-    }
-    if (on) {
-#pragma unroll
-      for (int r = 0; r < BY; ++r) {
-        A a[4];
-        ld4(ang + 2 * ((y0 + r) * L + x0), a);
-        // x-bond of (x0+c, y0+r) is in g1 when the site is an A site, else g3
-        tpx_[PHS ? 0 : r][0] = tphase((R)a[0], (r & 1) == 0 ? t1 : th);
-        tpy_[PHS ? 0 : r][0] = tphase((R)a[1], th);
-        tpx_[PHS ? 0 : r][1] = tphase((R)a[2], (r & 1) == 1 ? t1 : th);
-        tpy_[PHS ? 0 : r][1] = tphase((R)a[3], th);
-      }
-      if (!XS) {
-#pragma unroll
-        for (int r = 0; r < BY; ++r) phr[(y0 + r) * nbx + bx] = tpx_[PHS ? 0 : r][1];
-      }
-      phb[by * L + x0] = tpy_[PHS ? 0 : BY - 1][0];
-      phb[by * L + x0 + 1] = tpy_[PHS ? 0 : BY - 1][1];
-    }
-    if (XS) {
-#pragma unroll
-      for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = shfl_c(tpx_[PHS ? 0 : r][1], lane_l);
-    }
-    __syncthreads();
-    if (on) {
-      if (!XS) {
-#pragma unroll
-        for (int r = 0; r < BY; ++r) tpl_[PHS ? 0 : r] = phr[(y0 + r) * nbx + bxl];
-      }
-      tpt_[0] = phb[byu * L + x0];
-      tpt_[1] = phb[byu * L + x0 + 1];
+    } else {
+      A a[BY][4];
+      load_angles(a, ang);
+      phases_from(a, t1, th);
     }
   }
 
@@ -328,14 +318,12 @@ struct Slice {
       return;  // no shared-memory buffer used
     }
     if (G == 0 || G == 2) {
-      Cx<R>* xl = buf;
-      Cx<R>* xr = buf + L * nbx;
       if (on) {
 #pragma unroll
         for (int r = 0; r < BY; ++r)
           if (xcross(G, r)) {
-            xl[(y0 + r) * nbx + bx] = v[r][0];
-            xr[(y0 + r) * nbx + bx] = v[r][1];
+            slot(buf, r & ~1)[id] = v[r][0];
+            slot(buf, (r & ~1) + 1)[id] = v[r][1];
           }
       }
       __syncthreads();
@@ -345,8 +333,8 @@ struct Slice {
           if (!xcross(G, r)) {
             pair_update<MODE>(v[r][0], v[r][1], TPX(r, 0), c);
           } else {
-            const Cx<R> right = xl[(y0 + r) * nbx + bxr];
-            const Cx<R> left = xr[(y0 + r) * nbx + bxl];
+            const Cx<R> right = slot(buf, r & ~1)[idr];
+            const Cx<R> left = slot(buf, (r & ~1) + 1)[idl];
             Cx<R> ao = TPX(r, 1), al = TPL(r);
             if (MODE == FAC_INV) {
               ao = cneg(ao);
@@ -364,11 +352,9 @@ struct Slice {
     } else {
       constexpr int CL = (G == 1) ? 0 : 1;  // column with only local pairs
       constexpr int CC = 1 - CL;            // column with cross pairs at its ends
-      Cx<R>* yt = buf;
-      Cx<R>* yb = buf + nby * L;
       if (on) {
-        yt[by * L + x0 + CC] = v[0][CC];
-        yb[by * L + x0 + CC] = v[BY - 1][CC];
+        slot(buf, 0)[id] = v[0][CC];
+        slot(buf, 1)[id] = v[BY - 1][CC];
       }
       __syncthreads();
       if (on) {
@@ -376,8 +362,8 @@ struct Slice {
         for (int r = 0; r < BY; r += 2) pair_update<MODE>(v[r][CL], v[r + 1][CL], TPY(r, CL), c);
 #pragma unroll
         for (int r = 1; r + 1 < BY; r += 2) pair_update<MODE>(v[r][CC], v[r + 1][CC], TPY(r, CC), c);
-        const Cx<R> below = yt[byd * L + x0 + CC];
-        const Cx<R> above = yb[byu * L + x0 + CC];
+        const Cx<R> below = slot(buf, 0)[idd];
+        const Cx<R> above = slot(buf, 1)[idu];
         Cx<R> ab = TPY(BY - 1, CC), at = TPT(CC);
         if (MODE == FAC_INV) {
           ab = cneg(ab);
