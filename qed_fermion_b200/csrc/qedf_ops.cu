@@ -650,7 +650,8 @@ template int launch_precon<double>(const PreconArgs&, cudaStream_t);
 template <typename R, typename A, int BY, bool PHS>
 static int launch_force_t(const ForceArgs& a, cudaStream_t st) {
   const int threads = ((a.L / 2) * (a.L / BY) + 31) / 32 * 32;
-  const size_t smem = slice_smem_bytes<R, PHS ? EC_PHS : 0>(a.L, BY, 4);
+  // four exchange buffers; the force keeps no stash
+  const size_t smem = slice_smem_bytes<R, (PHS ? EC_PHS : 0) | EC_NOSTASH>(a.L, BY, 4);
   if (smem > smem_limit()) return QEDF_ERR_SIZE;
   if (prepare_smem(k_force<R, A, BY, PHS>, smem)) return QEDF_ERR_CUDA;
   dim3 grid((a.Nt + a.T - 1) / a.T, a.bs);
@@ -660,7 +661,7 @@ static int launch_force_t(const ForceArgs& a, cudaStream_t st) {
 
 template <typename R, typename A, int BY>
 static int launch_force_by(const ForceArgs& a, cudaStream_t st) {
-  if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS>(a.L, BY, 4) <= smem_limit())
+  if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS | EC_NOSTASH>(a.L, BY, 4) <= smem_limit())
     return launch_force_t<R, A, BY, true>(a, st);
   return launch_force_t<R, A, BY, false>(a, st);
 }

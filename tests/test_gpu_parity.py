@@ -138,8 +138,6 @@ def test_precon_vec_dropin(prec):
 @pytest.mark.parametrize("prec", ["c64", "c128"])
 def test_force_matches_oracle(prec, L, Nt, bs):
     from qed_fermion_b200 import ops
-    if prec == "c128" and L == 66:
-        pytest.skip("double-precision force at L=66 exceeds the shared-memory budget (mixed path uses float)")
     boson, xi = rand_case(L, Nt, bs, seed=11 + L)
     phi = O.ref_to_kernel_layout(boson)
     want = O.force_f_from_xi(phi, xi.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
