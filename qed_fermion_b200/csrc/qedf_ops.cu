@@ -31,9 +31,11 @@ __global__ void __launch_bounds__(MaxT<BY, EC>::value, MaxT<BY, EC>::min_blocks)
   constexpr bool PHS = (EC & EC_PHS) != 0;
   constexpr bool STASH = (EC & EC_NOSTASH) == 0;
   constexpr bool XS = (EC & EC_XS) != 0;
-  Slice<R, BY, PHS, XS> S;
-  S.init(p.L, smem, 2, (R)p.c1, (R)p.ch, threadIdx.x);
-  const int Vs = p.L * p.L;
+  constexpr int LT = ec_fixed_l(EC);
+  Slice<R, BY, PHS, XS, LT> S;
+  const int L = lattice_l<EC>(p.L);
+  S.init(L, smem, 2, (R)p.c1, (R)p.ch, threadIdx.x);
+  const int Vs = L * L;
   const size_t sv = 2 * (size_t)Vs;  // reals per slice (vector and angles)
   const int rb = blockIdx.y;
   const int a = blockIdx.x * p.T;
@@ -110,7 +112,7 @@ __global__ void __launch_bounds__(MaxT<BY, EC>::value, MaxT<BY, EC>::min_blocks)
         copy_blk<R, BY>(X0, Yp);
         copy_blk<R, BY>(Yp, Y);
       }
-      S.template applyB<FAC_TILDE>(Y);            // B_t y_{t+1}
+      S.template applyB<FAC_TILDE, 1>(Y);         // B_t y_{t+1}
       if (S.on) {
         axpy_blk<R, BY>(Y, X0, sg, Y);            // z_t = y_t - sigma_t B_t y_{t+1}
         S.store(z + t * sv, Y);
@@ -192,10 +194,11 @@ __global__ void k_precon(PreconArgs p) {
 // while l is advanced forwards, so no partial product is stored.  This is the
 // sum that the reference evaluates with explicit partial products
 // (force_f_fast, hmc_sampler_batch.py:2150-2227; force_f_sparse :2230-2330).
-template <typename R, typename A, int BY, bool PHS>
+template <typename R, typename A, int BY, bool PHS, int LT = 0>
 struct ForceSlice {
-  Slice<R, BY, PHS>& S;
-  __device__ ForceSlice(Slice<R, BY, PHS>& s) : S(s) {}
+  using Eng = Slice<R, BY, PHS, false, LT>;
+  Eng& S;
+  __device__ ForceSlice(Eng& s) : S(s) {}
 
   // term for one bond: c * [conj(l_i) (i a) R_j + conj(l_j) conj(i a) R_i]
   __device__ static __forceinline__ R term(Cx<R> li, Cx<R> lj, Cx<R> Ri, Cx<R> Rj, Cx<R> a, R c) {
@@ -218,7 +221,7 @@ struct ForceSlice {
       if (S.on) {
 #pragma unroll
         for (int r = 0; r < BY; ++r)
-          if (Slice<R, BY, PHS>::xcross(G, r)) {
+          if (Eng::xcross(G, r)) {
             S.slot(bR, r & ~1)[S.id] = Rv[r][0];
             S.slot(bR, (r & ~1) + 1)[S.id] = Rv[r][1];
             S.slot(bl, r & ~1)[S.id] = l[r][0];
@@ -229,7 +232,7 @@ struct ForceSlice {
       if (!S.on) return;
 #pragma unroll
       for (int r = 0; r < BY; ++r) {
-        if (!Slice<R, BY, PHS>::xcross(G, r)) {
+        if (!Eng::xcross(G, r)) {
           const Cx<R> a = S.TPX(r, 0);
           const Cx<R> Ri = Rv[r][0], Rj = Rv[r][1];
           const Cx<R> nRi = c * cfma(cneg(a), Rj, Ri);
@@ -316,13 +319,14 @@ struct ForceSlice {
   }
 };
 
-template <typename R, typename A, int BY, bool PHS>
+template <typename R, typename A, int BY, bool PHS, int LT = 0>
 __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_force(ForceArgs p) {
   extern __shared__ __align__(16) unsigned char smem[];
-  Slice<R, BY, PHS> S;
-  S.init(p.L, smem, 4, (R)p.c1, (R)p.ch, threadIdx.x);
-  ForceSlice<R, A, BY, PHS> FS(S);
-  const int Vs = p.L * p.L;
+  Slice<R, BY, PHS, false, LT> S;
+  const int L = LT ? LT : p.L;
+  S.init(L, smem, 4, (R)p.c1, (R)p.ch, threadIdx.x);
+  ForceSlice<R, A, BY, PHS, LT> FS(S);
+  const int Vs = L * L;
   const size_t sv = 2 * (size_t)Vs;
   const int rb = blockIdx.y;
   const int a = blockIdx.x * p.T;
@@ -356,7 +360,7 @@ __global__ void __launch_bounds__(MaxThreads<BY>::value, 1) k_force(ForceArgs p)
 #pragma unroll
       for (int r = 0; r < BY; ++r) {
         A o[4] = {(A)Fx[r][0], (A)Fy[r][0], (A)Fx[r][1], (A)Fy[r][1]};
-        st4(F + t * sv + 2 * ((S.y0 + r) * p.L + S.x0), o);
+        st4(F + t * sv + 2 * ((S.y0 + r) * L + S.x0), o);
       }
     }
     copy_blk<R, BY>(Rv, Xn);
@@ -577,18 +581,27 @@ static int launch_operator_t(int op, const OpArgs& a, cudaStream_t st) {
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
 
+// Lattice sides with engines compiled for a fixed L (the benchmark lattice,
+// L = 48); every other L runs the run-time-L engine.
+template <typename R, typename A, int BY, int EC>
+static int launch_operator_fl(int op, const OpArgs& a, cudaStream_t st) {
+  if constexpr (BY == 2 && (EC == 0 || EC == EC_PHS))
+    if (a.L == 48) return launch_operator_t<R, A, BY, EC | EC_L(48)>(op, a, st);
+  return launch_operator_t<R, A, BY, EC>(op, a, st);
+}
+
 // double precision keeps the phases in shared memory when they fit; without
 // room for the stash, y stays in registers
 template <typename R, typename A, int BY>
 static int launch_operator_by(int op, const OpArgs& a, int xs, cudaStream_t st) {
   if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
-    return launch_operator_t<R, A, BY, EC_PHS>(op, a, st);
+    return launch_operator_fl<R, A, BY, EC_PHS>(op, a, st);
   if (sizeof(R) == 4 && a.variant == 1 && 2 * slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
     return launch_operator_t<R, A, BY, EC_PHS | EC_2CTA>(op, a, st);
   if (sizeof(R) == 4 && xs && xs_possible(a.L) && ((a.L / 2) & (a.L / 2 - 1)) == 0 &&
       slice_threads(a.L, BY, true) <= MaxT<BY, EC_XS>::value)
     return launch_operator_t<R, A, BY, EC_XS>(op, a, st);
-  if (slice_smem_bytes<R, 0>(a.L, BY, 2) <= smem_limit()) return launch_operator_t<R, A, BY, 0>(op, a, st);
+  if (slice_smem_bytes<R, 0>(a.L, BY, 2) <= smem_limit()) return launch_operator_fl<R, A, BY, 0>(op, a, st);
   return launch_operator_t<R, A, BY, EC_NOSTASH>(op, a, st);
 }
 
@@ -647,22 +660,26 @@ int launch_precon(const PreconArgs& a, cudaStream_t st) {
 template int launch_precon<float>(const PreconArgs&, cudaStream_t);
 template int launch_precon<double>(const PreconArgs&, cudaStream_t);
 
-template <typename R, typename A, int BY, bool PHS>
+template <typename R, typename A, int BY, bool PHS, int LT = 0>
 static int launch_force_t(const ForceArgs& a, cudaStream_t st) {
   const int threads = ((a.L / 2) * (a.L / BY) + 31) / 32 * 32;
   // four exchange buffers; the force keeps no stash
   const size_t smem = slice_smem_bytes<R, (PHS ? EC_PHS : 0) | EC_NOSTASH>(a.L, BY, 4);
   if (smem > smem_limit()) return QEDF_ERR_SIZE;
-  if (prepare_smem(k_force<R, A, BY, PHS>, smem)) return QEDF_ERR_CUDA;
+  if (prepare_smem(k_force<R, A, BY, PHS, LT>, smem)) return QEDF_ERR_CUDA;
   dim3 grid((a.Nt + a.T - 1) / a.T, a.bs);
-  k_force<R, A, BY, PHS><<<grid, threads, smem, st>>>(a);
+  k_force<R, A, BY, PHS, LT><<<grid, threads, smem, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
 
 template <typename R, typename A, int BY>
 static int launch_force_by(const ForceArgs& a, cudaStream_t st) {
-  if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS | EC_NOSTASH>(a.L, BY, 4) <= smem_limit())
+  // the benchmark lattice L = 48 runs an engine compiled for it
+  if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS | EC_NOSTASH>(a.L, BY, 4) <= smem_limit()) {
+    if (BY == 2 && a.L == 48) return launch_force_t<R, A, BY, true, 48>(a, st);
     return launch_force_t<R, A, BY, true>(a, st);
+  }
+  if (BY == 2 && a.L == 48) return launch_force_t<R, A, BY, false, 48>(a, st);
   return launch_force_t<R, A, BY, false>(a, st);
 }
 

@@ -186,6 +186,9 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   extern __shared__ __align__(16) unsigned char dsm[];
   __shared__ RhsState st;
   constexpr bool MIXED = !std::is_same<RS, RH>::value;
+  // lattice side: compiled in (every system has it) or per system
+  constexpr int LT = ec_fixed_l(ECS);
+  auto SL = [](const PcgSys& S) { return LT ? LT : S.L; };
   const int NV = p.nrhs;
   Acc acc(p.acc, NV);
   const unsigned int nblk = gridDim.x;
@@ -218,13 +221,13 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const PcgSys& S = p.sys[s];
     const int lu = u - S.unitE0;
     v = S.rhs0 + lu / S.nchunk;
-    const int Vs = S.L * S.L;
+    const int Vs = SL(S) * SL(S);
     c0 = (lu % S.nchunk) * CH;
     c1 = min(c0 + CH, Vs);
   };
   auto vec_base = [&](int s, int v) -> int64_t {
     const PcgSys& S = p.sys[s];
-    return S.vec0 + (int64_t)(v - S.rhs0) * S.Nt * S.L * S.L;
+    return S.vec0 + (int64_t)(v - S.rhs0) * S.Nt * SL(S) * SL(S);
   };
 
   // ---- BC-type elementwise pass over one unit --------------------------------
@@ -239,7 +242,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     int s, v, c0, c1;
     unitE(u, s, v, c0, c1);
     const PcgSys& S = p.sys[s];
-    const int Vs = S.L * S.L, Nt = S.Nt, w = c1 - c0;
+    const int Vs = SL(S) * SL(S), Nt = S.Nt, w = c1 - c0;
     const int64_t base = vec_base(s, v);
     Cx<RS>* rsm = reinterpret_cast<Cx<RS>*>(dsm);
     const RS al = (RS)st.alpha[v];
@@ -335,10 +338,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const int v = S.rhs0 + lu / S.nslab;
     const int a = (lu % S.nslab) * S.T;
     const int bnd = min(a + S.T, S.Nt);
-    const int Nt = S.Nt, Vs = S.L * S.L;
+    const int Nt = S.Nt, Vs = SL(S) * SL(S);
     const size_t sv = 2 * (size_t)Vs;
-    Slice<RS, BY, PHS_S, XS_S> E;
-    E.init(S.L, dsm, 2, (RS)p.c1, (RS)p.ch, tid);
+    Slice<RS, BY, PHS_S, XS_S, LT> E;
+    E.init(SL(S), dsm, 2, (RS)p.c1, (RS)p.ch, tid);
     const int64_t vb = 2 * vec_base(s, v);  // reals
     const A* phi = phi_all + S.phi0 + (S.shared ? 0 : (int64_t)(v - S.rhs0) * Nt * sv);
     const RS beta = (RS)st.beta[v];
@@ -403,7 +406,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
 #pragma unroll
           for (int c = 0; c < 2; ++c) pap += (double)X0[q][c].re * X0[q][c].re + (double)X0[q][c].im * X0[q][c].im;
       }
-      E.template applyB<FAC_TILDE>(Y);        // B_t y_{t+1}
+      E.template applyB<FAC_TILDE, 1>(Y);     // B_t y_{t+1}
       if (E.on) {
         axpy_blk<RS, BY>(Y, X0, sg, Y);        // (M^dag M p)_t
         E.store(O + t * sv, Y);
@@ -423,10 +426,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const int v = S.rhs0 + lu / S.nslab;
     const int a = (lu % S.nslab) * S.T;
     const int bnd = min(a + S.T, S.Nt);
-    const int Nt = S.Nt, Vs = S.L * S.L;
+    const int Nt = S.Nt, Vs = SL(S) * SL(S);
     const size_t sv = 2 * (size_t)Vs;
-    Slice<RH, BY, PHS_H> E;
-    E.init(S.L, dsm, 2, (RH)p.c1, (RH)p.ch, tid);
+    Slice<RH, BY, PHS_H, false, LT> E;
+    E.init(SL(S), dsm, 2, (RH)p.c1, (RH)p.ch, tid);
     const int64_t vb = 2 * vec_base(s, v);
     const A* phi = phi_all + S.phi0 + (S.shared ? 0 : (int64_t)(v - S.rhs0) * Nt * sv);
     const RH* xx = xh + vb;
@@ -460,7 +463,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         copy_blk<RH, BY>(X0, Yp);
         copy_blk<RH, BY>(Yp, Y);
       }
-      E.template applyB<FAC_TILDE>(Y);
+      E.template applyB<FAC_TILDE, 1>(Y);
       if (E.on) {
         axpy_blk<RH, BY>(Y, X0, sg, Y);  // (A x)_t
         E.load_coherent(X0, bb + t * sv);
@@ -470,7 +473,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
           for (int c = 0; c < 2; ++c) {
             const RH dr = X0[q][c].re - Y[q][c].re, di = X0[q][c].im - Y[q][c].im;
             rr_acc += (double)dr * dr + (double)di * di;
-            const int64_t site = (int64_t)t * Vs + (E.y0 + q) * S.L + E.x0 + c;
+            const int64_t site = (int64_t)t * Vs + (E.y0 + q) * SL(S) + E.x0 + c;
             rout[2 * site] = (RS)dr;
             rout[2 * site + 1] = (RS)di;
           }
@@ -488,7 +491,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     unitE(u, s, v, c0, c1);
     if (!(all_active ? st.active[v] : st.ru[v])) return;
     const PcgSys& S = p.sys[s];
-    const int Vs = S.L * S.L, w = c1 - c0;
+    const int Vs = SL(S) * SL(S), w = c1 - c0;
     const int64_t base = vec_base(s, v);
     const int j = tid % PPR;
     if (2 * j >= w) return;
@@ -820,6 +823,17 @@ int launch_pcg_prep(const PcgParams& p, int zero_words, cudaStream_t st) {
 
 static bool fits(size_t engine_bytes) { return engine_bytes + sizeof(RhsState) <= 227 * 1024; }
 
+// Engines compiled for a fixed lattice side (the benchmark lattice, L = 48)
+// when every system has it; otherwise the run-time-L engine.
+template <typename RS, typename RH, typename A, int BY, int ECS, int ECH>
+static int launch_pcg_fl(PcgParams& p, cudaStream_t st) {
+  bool all48 = BY == 2;
+  for (int s = 0; s < p.nsys; ++s) all48 = all48 && p.sys[s].L == 48;
+  if constexpr (BY == 2)
+    if (all48) return launch_pcg_t<RS, RH, A, BY, ECS | EC_L(48), ECH | EC_L(48)>(p, st);
+  return launch_pcg_t<RS, RH, A, BY, ECS, ECH>(p, st);
+}
+
 template <int BY>
 static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
   int Lmax = 0;
@@ -839,11 +853,11 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
       if (xs && fits(slice_smem_bytes<float, 0>(Lmax, BY, 2)))
         return launch_pcg_t<float, float, float, BY, EC_XS, EC_XS>(p, st);
       if (fits(slice_smem_bytes<float, 0>(Lmax, BY, 2)))
-        return launch_pcg_t<float, float, float, BY, 0, 0>(p, st);
+        return launch_pcg_fl<float, float, float, BY, 0, 0>(p, st);
       return launch_pcg_t<float, float, float, BY, EC_NOSTASH, EC_NOSTASH>(p, st);
     case QEDF_PCG_PLAIN_F64:
       if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
-        return launch_pcg_t<double, double, double, BY, EC_PHS, EC_PHS>(p, st);
+        return launch_pcg_fl<double, double, double, BY, EC_PHS, EC_PHS>(p, st);
       if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
         return launch_pcg_t<double, double, double, BY, 0, 0>(p, st);
       return launch_pcg_t<double, double, double, BY, EC_NOSTASH, EC_NOSTASH>(p, st);
@@ -853,7 +867,7 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
       if (xs && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
         return launch_pcg_t<float, double, float, BY, EC_XS, EC_PHS>(p, st);
       if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
-        return launch_pcg_t<float, double, float, BY, 0, EC_PHS>(p, st);
+        return launch_pcg_fl<float, double, float, BY, 0, EC_PHS>(p, st);
       if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
         return launch_pcg_t<float, double, float, BY, 0, 0>(p, st);
       return launch_pcg_t<float, double, float, BY, 0, EC_NOSTASH>(p, st);

@@ -49,7 +49,16 @@ struct MaxThreads {
 //              whole rows of tiles (L/2 <= 32 tiles per row, padded to a power
 //              of two), so only the y-bond factors need a block barrier
 //   EC_2CTA    compiled for two resident blocks per SM (register budget halved)
+//   EC_L(l)    (bits 8 and up) the lattice side fixed at compile time, so the
+//              engine's index arithmetic folds into constants; 0 = run-time L
 enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_2CTA = 8 };
+__host__ __device__ constexpr int EC_L(int l) { return l << 8; }
+__host__ __device__ constexpr int ec_fixed_l(int ec) { return ec >> 8; }
+// the lattice side of a kernel compiled for engine configuration EC
+template <int EC>
+__host__ __device__ __forceinline__ int lattice_l(int runtime_l) {
+  return ec_fixed_l(EC) ? ec_fixed_l(EC) : runtime_l;
+}
 
 // Largest thread block of a kernel compiled for tile height BY and engine
 // configuration EC (it fixes the register budget: 65536 / value per thread).
@@ -84,7 +93,7 @@ __host__ __device__ inline size_t slice_smem_bytes(int L, int BY, int nbuf) {
   return sizeof(Cx<R>) * (nbuf * BY * NT + ph + ((EC & EC_NOSTASH) ? 0 : 2 * BY * NT));
 }
 
-template <typename R, int BY, bool PHS = false, bool XS = false>
+template <typename R, int BY, bool PHS = false, bool XS = false, int LT = 0>
 struct Slice {
   static_assert(BY % 2 == 0, "BY must be even");
   int L, nbx, nby, NT, bx, by, x0, y0, bxl, bxr, byu, byd;
@@ -120,7 +129,7 @@ struct Slice {
 
   // smem must hold slice_smem_bytes<R, EC>(L, BY, nbuf) for the kernel's EC
   __device__ void init(int L_, unsigned char* smem, int nbuf, R c1_, R ch_, int tid) {
-    L = L_;
+    L = LT ? LT : L_;
     nbx = L / 2;
     nby = L / BY;
     NT = nbx * nby;
@@ -287,10 +296,12 @@ struct Slice {
     }
   }
 
-  template <int G, int MODE>
+  // BUF: exchange buffer 0 or 1 fixed at compile time, or -1 for the
+  // alternating run-time choice
+  template <int G, int MODE, int BUF = -1>
   __device__ __forceinline__ void factor(Cx<R> (&v)[BY][2]) {
     const R c = (G == 0) ? c1 : ch;
-    Cx<R>* buf = cur ? xb[1] : xb[0];
+    Cx<R>* buf = BUF >= 0 ? xb[BUF] : (cur ? xb[1] : xb[0]);
     if (XS && (G == 0 || G == 2)) {
       // neighbours' old values by shuffle; every lane takes part
 #pragma unroll
@@ -379,19 +390,21 @@ struct Slice {
         v[0][CC] = nt;
       }
     }
-    cur ^= 1;
+    if (BUF < 0) cur ^= 1;
   }
 
-  // B = F4 F3 F2 F1 F2 F3 F4 without the scalar Cb (FAC_TILDE) or exact
-  template <int MODE>
+  // B = F4 F3 F2 F1 F2 F3 F4 without the scalar Cb (FAC_TILDE) or exact.
+  // The seven factors use exchange buffers P, 1-P, ..., P; two applications in
+  // a row must alternate P (or be separated by a barrier).
+  template <int MODE, int P = 0>
   __device__ __forceinline__ void applyB(Cx<R> (&v)[BY][2]) {
-    factor<3, MODE>(v);
-    factor<2, MODE>(v);
-    factor<1, MODE>(v);
-    factor<0, MODE>(v);
-    factor<1, MODE>(v);
-    factor<2, MODE>(v);
-    factor<3, MODE>(v);
+    factor<3, MODE, P>(v);
+    factor<2, MODE, 1 - P>(v);
+    factor<1, MODE, P>(v);
+    factor<0, MODE, 1 - P>(v);
+    factor<1, MODE, P>(v);
+    factor<2, MODE, 1 - P>(v);
+    factor<3, MODE, P>(v);
   }
 };
 
