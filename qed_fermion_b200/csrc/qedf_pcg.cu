@@ -100,6 +100,27 @@ __device__ double block_sum_d(double v, double* sh) {
   return t;
 }
 
+// three sums over the block at once, results valid in thread 0 (sh: 96 doubles)
+__device__ void block_sum3_d(double& a, double& b, double& c, double* sh) {
+  a = warp_sum_d(a);
+  b = warp_sum_d(b);
+  c = warp_sum_d(c);
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  __syncthreads();
+  if (ln == 0) {
+    sh[w] = a;
+    sh[32 + w] = b;
+    sh[64 + w] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const bool in = threadIdx.x < (blockDim.x + 31) / 32;
+    a = warp_sum_d(in ? sh[threadIdx.x] : 0.0);
+    b = warp_sum_d(in ? sh[32 + threadIdx.x] : 0.0);
+    c = warp_sum_d(in ? sh[64 + threadIdx.x] : 0.0);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // accumulator layout (doubles)
 // ---------------------------------------------------------------------------
@@ -150,7 +171,7 @@ struct RhsState {
   int iters[PCG_MAX_RHS], lastru[PCG_MAX_RHS], status[PCG_MAX_RHS];
   unsigned char active[PCG_MAX_RHS], ru[PCG_MAX_RHS];
   int any_active, any_ru;
-  double red[32];
+  double red[96];
 };
 
 // Optional phase timing (block 0, thread 0): prof[k] accumulates clock64 cycles of
@@ -310,9 +331,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       }
       acc_b += (double)r0.re * z0.re + (double)r0.im * z0.im + (double)r1.re * z1.re + (double)r1.im * z1.im;
     }
-    const double sa = block_sum_d(acc_a, st.red);
-    const double sb = block_sum_d(acc_b, st.red);
-    const double sc = block_sum_d(acc_c, st.red);
+    double sa = acc_a, sb = acc_b, sc = acc_c;
+    block_sum3_d(sa, sb, sc, st.red);
     if (tid == 0) {
       if (kind == 0) {
         atomicAdd(acc.bb + v, sa);
@@ -401,10 +421,12 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         copy_blk<RS, BY>(Yp, Y);
       }
       if (E.on) {
+        RS sq = 0;  // the tile's |y_t|^2 in the iteration precision, then double
 #pragma unroll
         for (int q = 0; q < BY; ++q)
 #pragma unroll
-          for (int c = 0; c < 2; ++c) pap += (double)X0[q][c].re * X0[q][c].re + (double)X0[q][c].im * X0[q][c].im;
+          for (int c = 0; c < 2; ++c) sq = fma(X0[q][c].re, X0[q][c].re, fma(X0[q][c].im, X0[q][c].im, sq));
+        pap += (double)sq;
       }
       E.template applyB<FAC_TILDE, 1>(Y);     // B_t y_{t+1}
       if (E.on) {

@@ -144,7 +144,10 @@ struct Slice {
       lane_l = on ? seg * W + (tbx == 0 ? nbx - 1 : tbx - 1) : lane;
       lane_r = on ? seg * W + (tbx + 1 == nbx ? 0 : tbx + 1) : lane;
     } else {
-      on = tid < NT;
+      // a fixed L whose tiles fill whole warps is launched with one thread per
+      // tile exactly, so every thread owns a tile
+      constexpr bool ALL_ON = LT > 0 && ((LT / 2) * (LT / BY)) % 32 == 0;
+      on = ALL_ON || tid < NT;
       bx = on ? tid % nbx : 0;
       by = on ? tid / nbx : 0;
       lane_l = lane_r = 0;

@@ -70,6 +70,22 @@ def test_operator_matches_oracle(op, prec, L, Nt, bs, by, slab):
     assert relerr(got.cpu().numpy(), want) < tol
 
 
+@pytest.mark.parametrize("L,Nt,bs,slab,rpp", [(48, 8, 2, 0, 1), (48, 6, 4, 2, 1), (24, 10, 2, 3, 1),
+                                               (6, 20, 2, 1, 1), (10, 7, 4, 0, 2), (48, 5, 2, 0, 2)])
+def test_mhm_multi_rhs_fields_match_oracle(L, Nt, bs, slab, rpp):
+    """complex64 M^dag M on several vectors with their own fields or groups of
+    vectors sharing one field, including the engine compiled for L = 48."""
+    from qed_fermion_b200 import ops
+    boson, v = rand_case(L, Nt, bs, seed=L * 7 + bs)
+    boson = np.repeat(boson[::rpp], rpp, axis=0)
+    phi = O.ref_to_kernel_layout(boson)
+    want = O.mhm_vec(phi, v.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    got = ops.apply_operator("mhm", torch.tensor(phi[::rpp].reshape(bs // rpp, -1), dtype=torch.float32, device=DEV),
+                             torch.tensor(v, dtype=torch.complex64, device=DEV), L, 0.1, slab=slab,
+                             rhs_per_boson=rpp)
+    assert relerr(got.cpu().numpy(), want) < 1e-6
+
+
 @pytest.mark.parametrize("prec", ["c64", "c128"])
 def test_operator_shared_boson_rows(prec):
     """Several vectors referencing one angle array (the estimator's layout)."""
