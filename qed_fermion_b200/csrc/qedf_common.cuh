@@ -133,6 +133,17 @@ __device__ __forceinline__ void st4(double* p, const double (&a)[4]) {
   reinterpret_cast<double2*>(p)[1] = make_double2(a[2], a[3]);
 }
 
+// Asynchronous 16-byte copies global -> shared, cached in L2 only (data that
+// other SMs wrote before a grid barrier is seen).  Both addresses are 16-byte
+// aligned.  cp_async_wait<N>: at most the N most recent groups still pending.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Coefficients of the checkerboard factors F_g = c_g (I + t_g K_g):
 // g1 uses cosh/tanh(dtau), g2..g4 cosh/tanh(dtau/2); Cb = c1 c2^2 c3^2 c4^2
 // is the scalar that B = F4 F3 F2 F1 F2 F3 F4 carries in front of the

@@ -102,6 +102,7 @@ struct PcgSys {
   int64_t phi0;          // first real of the system in the packed angles
   int precon;
   int ptab0;             // first entry of the system's preconditioner band table
+  int pmid_lo, pmid_hi;  // rows [lo, hi) of the preconditioner that are the bulk band
 };
 
 struct PcgParams {

@@ -273,6 +273,49 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const int rstep = blockDim.x / PPR;
     const bool jon = 2 * j < w;
     double acc_a = 0, acc_b = 0, acc_c = 0;
+    if (sizeof(RS) == 4 && kind == 1) {
+      // The iteration update, single precision: the four input rows (p, Op,
+      // x, r) of this thread's next two rows are in flight while one row is
+      // updated, as 16-byte cp.async copies into a two-stage area behind the
+      // unit's r column (stage k & 1, [vector][thread] units).  A stage is
+      // refilled only after its values were used.
+      uint4* stg = reinterpret_cast<uint4*>(dsm + ((size_t)Nt * CHC * sizeof(Cx<RS>) + 15) / 16 * 16);
+      const int nthr = blockDim.x, t0 = tid / PPR;
+      const int K = (jon && t0 < Nt) ? (Nt - 1 - t0) / rstep + 1 : 0;
+      RS cpart = 0;  // this thread's |r|^2 in the iteration precision
+      auto issue = [&](int k) {
+        const int64_t i2 = 2 * (base + (int64_t)(t0 + k * rstep) * Vs + c0 + 2 * j);
+        uint4* d = stg + (size_t)(k & 1) * 4 * nthr + tid;
+        cp_async16(d, pn + i2);
+        cp_async16(d + nthr, opv + i2);
+        cp_async16(d + 2 * nthr, xs + i2);
+        cp_async16(d + 3 * nthr, r + i2);
+        cp_async_commit();
+      };
+      if (K > 0) issue(0);
+      if (K > 1) issue(1);
+      for (int k = 0; k < K; ++k) {
+        if (k + 1 < K) cp_async_wait<1>(); else cp_async_wait<0>();
+        const RS* d = reinterpret_cast<const RS*>(stg + (size_t)(k & 1) * 4 * nthr + tid);
+        Cx<RS> p0v, p1v, o0, o1, x0, x1, r0, r1;
+        ld2c(d, p0v, p1v);
+        ld2c(d + 4 * nthr, o0, o1);
+        ld2c(d + 8 * nthr, x0, x1);
+        ld2c(d + 12 * nthr, r0, r1);
+        x0 = mk<RS>(fma(al, p0v.re, x0.re), fma(al, p0v.im, x0.im));
+        x1 = mk<RS>(fma(al, p1v.re, x1.re), fma(al, p1v.im, x1.im));
+        r0 = mk<RS>(fma(-al, o0.re, r0.re), fma(-al, o0.im, r0.im));
+        r1 = mk<RS>(fma(-al, o1.re, r1.re), fma(-al, o1.im, r1.im));
+        const int t = t0 + k * rstep;
+        const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
+        st2(xs + i2, x0, x1);
+        st2(r + i2, r0, r1);
+        cpart = fma(r0.re, r0.re, fma(r0.im, r0.im, fma(r1.re, r1.re, fma(r1.im, r1.im, cpart))));
+        st2(reinterpret_cast<RS*>(rsm + t * CHC + 2 * j), r0, r1);
+        if (k + 2 < K) issue(k + 2);
+      }
+      acc_c += (double)cpart;
+    } else
 #pragma unroll 2
     for (int t = tid / PPR; t < Nt; t += rstep) {
       if (!jon) continue;
@@ -307,6 +350,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     }
     __syncthreads();
     const float* tab = p.ptab + S.ptab0;
+    RS cmid[7];  // the bulk band, by tau distance
+#pragma unroll
+    for (int d = 0; d < 7; ++d) cmid[d] = (RS)c_pre.middle[d];
+    RS bpart = 0;  // this thread's r^dag z in the iteration precision
 #pragma unroll 2
     for (int t = tid / PPR; t < Nt; t += rstep) {
       if (!jon) continue;
@@ -316,21 +363,34 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       if (S.precon) {
         z0 = mk<RS>(0, 0);
         z1 = mk<RS>(0, 0);
-        int tt = t - 6 < 0 ? t - 6 + Nt : t - 6;
+        if (t >= S.pmid_lo && t < S.pmid_hi) {
+          // bulk row: coefficients in registers, no wrap (t - 6 >= 0, t + 6 < Nt)
 #pragma unroll
-        for (int k = 0; k < 13; ++k) {
-          const RS c = (RS)__ldg(tab + t * 13 + k);
-          Cx<RS> q0, q1;
-          ld2c(reinterpret_cast<const RS*>(rsm + tt * CHC + 2 * j), q0, q1);
-          z0 = mk<RS>(fma(c, q0.re, z0.re), fma(c, q0.im, z0.im));
-          z1 = mk<RS>(fma(c, q1.re, z1.re), fma(c, q1.im, z1.im));
-          tt = tt + 1 == Nt ? 0 : tt + 1;
+          for (int k = 0; k < 13; ++k) {
+            const RS c = cmid[k < 6 ? 6 - k : k - 6];
+            Cx<RS> q0, q1;
+            ld2c(reinterpret_cast<const RS*>(rsm + (t - 6 + k) * CHC + 2 * j), q0, q1);
+            z0 = mk<RS>(fma(c, q0.re, z0.re), fma(c, q0.im, z0.im));
+            z1 = mk<RS>(fma(c, q1.re, z1.re), fma(c, q1.im, z1.im));
+          }
+        } else {
+          int tt = t - 6 < 0 ? t - 6 + Nt : t - 6;
+#pragma unroll
+          for (int k = 0; k < 13; ++k) {
+            const RS c = (RS)__ldg(tab + t * 13 + k);
+            Cx<RS> q0, q1;
+            ld2c(reinterpret_cast<const RS*>(rsm + tt * CHC + 2 * j), q0, q1);
+            z0 = mk<RS>(fma(c, q0.re, z0.re), fma(c, q0.im, z0.im));
+            z1 = mk<RS>(fma(c, q1.re, z1.re), fma(c, q1.im, z1.im));
+            tt = tt + 1 == Nt ? 0 : tt + 1;
+          }
         }
         const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
         st2(z + i2, z0, z1);
       }
-      acc_b += (double)r0.re * z0.re + (double)r0.im * z0.im + (double)r1.re * z1.re + (double)r1.im * z1.im;
+      bpart = fma(r0.re, z0.re, fma(r0.im, z0.im, fma(r1.re, z1.re, fma(r1.im, z1.im, bpart))));
     }
+    acc_b += (double)bpart;
     double sa = acc_a, sb = acc_b, sc = acc_c;
     block_sum3_d(sa, sb, sc, st.red);
     if (tid == 0) {
@@ -731,6 +791,28 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
       const int per_rhs = std::max(1, nblk / std::max(1, total_rhs));
       S.T = std::max(1, (q.Ltau + per_rhs - 1) / per_rhs);
     }
+    // the preconditioner rows that are the bulk band (middle values at every
+    // distance, nothing else): one contiguous range away from both tau ends
+    S.pmid_lo = S.pmid_hi = 0;
+    if (S.precon) {
+      int lo = -1, hi = -1;
+      for (int t = 0; t < q.Ltau; ++t) {
+        bool mid = t >= 6 && t + 6 < q.Ltau;
+        int cnt = 0;
+        pre_row(h_pre, q.Ltau, t, [&](int c, float val) {
+          const int d = c > t ? c - t : t - c;
+          mid = mid && d <= 6 && val == h_pre.middle[d];
+          ++cnt;
+        });
+        mid = mid && cnt == 13;
+        if (mid && lo < 0) lo = t;
+        if (mid) hi = t + 1;
+      }
+      if (lo >= 0) {
+        S.pmid_lo = lo;
+        S.pmid_hi = hi;
+      }
+    }
     S.nslab = (q.Ltau + S.T - 1) / S.T;
     S.nchunk = (q.Lx * q.Lx + p.CH - 1) / p.CH;
     S.rhs0 = rhs;
@@ -815,7 +897,10 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   const int threads = std::min(MaxT<BY, ECS>::value, std::max(128, eng_threads));
   size_t smem = slice_smem_bytes<RS, ECS>(Lmax, BY, 2);
   smem = std::max(smem, slice_smem_bytes<RH, ECH>(Lmax, BY, 2));
-  smem = std::max(smem, sizeof(Cx<RS>) * (size_t)Ntmax * PCG_CHUNK);
+  // elementwise units: the r column, and in single precision the two-stage
+  // area of the update pass
+  smem = std::max(smem, ((sizeof(Cx<RS>) * (size_t)Ntmax * PCG_CHUNK + 15) / 16 * 16) +
+                            (sizeof(RS) == 4 ? 2 * 4 * 16 * (size_t)threads : 0));
   if (smem + sizeof(RhsState) > 227 * 1024) return QEDF_ERR_SIZE;
   auto kern = k_pcg<RS, RH, A, BY, ECS, ECH>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
