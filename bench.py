@@ -33,6 +33,11 @@ if ROOT not in sys.path:
 
 METRIC = "HMC trajectories/hour at L=48, Ltau=480 (mixed precision, Delta H checked against FP64)"
 UNIT = "trajectories/hour"
+# DRAM bytes (read + write) per site and PCG iteration of k_pcg on this
+# workload, mixed precision, 2 right-hand sides: ncu --metrics
+# dram__bytes_read.sum,dram__bytes_write.sum of `bench.py --solve-only 482`
+# (profiles/k_pcg_mixed_L48_Lt480_rhs2.md)
+PCG_DRAM_BYTES_PER_SITE_ITER = 71.1
 
 
 def parse_args(argv=None):
@@ -337,6 +342,11 @@ def run_native(args):
         pcg_bytes.append(it_sum * N * (7 * 8 + 2 * 4))  # float vectors and angles per iteration
     pcg_time = sum(pcg_ms) / 1e3
     achieved = sum(pcg_bytes) / pcg_time / 1e9 if pcg_time > 0 else None
+    # DRAM traffic per launch: bytes per site and iteration from one ncu capture
+    # of a full-length solve of this workload, scaled by the site-iterations of
+    # the average launch here
+    site_iters = statistics.mean(b / (7 * 8 + 2 * 4) for b in pcg_bytes) if pcg_bytes else 0
+    traffic = PCG_DRAM_BYTES_PER_SITE_ITER * site_iters if site_iters else None
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -472,7 +482,11 @@ def run_native(args):
             "roofline": {"bound": "hbm", "kernel": "k_pcg (persistent batched PCG)",
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": (achieved / hbm_peak) if achieved else None, "peak_kind": peak_kind,
-                         "traffic": None,
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_launch": statistics.mean(pcg_bytes) if pcg_bytes else None,
+                         "traffic_source": f"dram__bytes_read+write of k_pcg, {PCG_DRAM_BYTES_PER_SITE_ITER} B per "
+                                           "site-iteration from an ncu capture of a 482-iteration solve of this "
+                                           "workload, times the average launch's site-iterations",
                          "bytes_model": "per PCG iteration per rhs: N*(7*8 + 2*4) B (read p,x,r,angles; write x,r,p)"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "fp64_plain": fp64, "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
