@@ -20,6 +20,7 @@ Precision ("precision" argument):
 from __future__ import annotations
 
 import math
+import os
 
 import torch
 
@@ -106,6 +107,66 @@ class HmcSampler:
         else:
             self.boson = stag
         return self.boson
+
+    # ---- boson checkpoints (reference :971-1016, :3164-3181, :3211-3215) -------
+    # The reference saves {'boson': [bs, 2, Lx, Ly, Ltau] on the CPU,
+    # 'delta_t_tensor': [bs]} with torch.save as "<folder>/<name>.pt", and reads
+    # either that dict or a bare boson tensor back.
+    def save_boson_checkpoint(self, data_folder, file_name):
+        """Write the current field and step sizes in the reference's format and
+        return the file path (``<data_folder>/<file_name>.pt``)."""
+        if self.boson is None:
+            raise RuntimeError("no boson field to save")
+        os.makedirs(data_folder, exist_ok=True)
+        path = os.path.join(data_folder, f"{file_name}.pt")
+        # the reference keeps delta_t_tensor in its field dtype
+        torch.save({"boson": self.boson.detach().cpu(),
+                    "delta_t_tensor": self.delta_t_tensor.detach().to(self.dtype).cpu()}, path)
+        return path
+
+    def load_boson_checkpoint(self, path):
+        """Read a field written by the reference or by ``save_boson_checkpoint``
+        (a dict with 'boson' and optionally 'delta_t_tensor', or a bare tensor)."""
+        loaded = torch.load(path, map_location="cpu")
+        boson = loaded["boson"] if isinstance(loaded, dict) else loaded
+        if tuple(boson.shape[1:]) != (2, self.Lx, self.Ly, self.Ltau):
+            raise RuntimeError(f"checkpoint field has shape {tuple(boson.shape)}, expected [bs, 2, {self.Lx}, "
+                               f"{self.Ly}, {self.Ltau}]")
+        self.boson = boson.to(device=self.device, dtype=self.dtype)
+        if isinstance(loaded, dict) and "delta_t_tensor" in loaded:
+            self.delta_t_tensor = loaded["delta_t_tensor"].to(device=self.device, dtype=torch.float64)
+        return self.boson
+
+    def initialize_boson_ensemble(self, data_folder, specifics, steps=range(4000, 10001, 500)):
+        """Warm start from saved ensemble members (reference :971-1016): the
+        files ``boson_<specifics>_<step>.pt`` that exist in ``data_folder``; one
+        field and one step-size tensor are drawn at random with the sampler's
+        generator.  Without any file the pi-flux start is used."""
+        bosons, dts = [], []
+        for step in steps:
+            path = os.path.join(data_folder, f"boson_{specifics}_{step}.pt")
+            if not os.path.exists(path):
+                continue
+            loaded = torch.load(path, map_location="cpu")
+            if isinstance(loaded, dict):
+                bosons.append(loaded["boson"])
+                if "delta_t_tensor" in loaded:
+                    dts.append(loaded["delta_t_tensor"])
+            else:
+                bosons.append(loaded)
+        if not bosons:
+            return self.initialize_boson_pi_flux_randn_matfree()
+        pick = int(torch.randint(len(bosons), (1,), generator=self._cpu_generator()).item())
+        self.boson = bosons[pick].to(device=self.device, dtype=self.dtype)
+        if dts:
+            pick = int(torch.randint(len(dts), (1,), generator=self._cpu_generator()).item())
+            self.delta_t_tensor = dts[pick].to(device=self.device, dtype=torch.float64)
+        return self.boson
+
+    def _cpu_generator(self):
+        g = torch.Generator()
+        g.manual_seed(int(torch.randint(0, 2 ** 31 - 1, (1,), device=self.device, generator=self.generator).item()))
+        return g
 
     # ---- random draws (reference :1247-1252, :1279-1287) ----------------------
     def draw_momentum(self):
