@@ -60,6 +60,8 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--solve-only", type=int, default=0,
                     help="profiling mode: one PCG solve of the workload with exactly this many iterations")
+    ap.add_argument("--configs", action="store_true",
+                    help="time the other benchmark configurations (C2, C4a, C4b, C5), one JSON line each")
     ap.add_argument("--matvec-only", type=int, default=0,
                     help="only time M^dag M on this many right-hand sides (c64; c128 with --mode fp64)")
     ap.add_argument("--mode", default="mixed", choices=["mixed", "fp32", "fp64"],
@@ -534,6 +536,88 @@ def run_solve_only(args):
     return 0
 
 
+def run_configs(args):
+    """The benchmark's other configurations on one GPU, each after a warm-up
+    run and timed with CUDA events: C2 (L=24 matvec and PCG to 1e-8 in both
+    precisions), C4a (64 Z2 noise vectors on one L=36 field), C4b (16 lattices
+    of uneven size in one launch), C5 (one 30-step trajectory at L=66)."""
+    import numpy as np
+    import torch
+    from qed_fermion_b200 import build, ops
+    from qed_fermion_b200.estimator import StochaticEstimator
+    from qed_fermion_b200.hmc import HmcSampler, ref_to_kernel
+    from qed_fermion_b200.solver import PcgSolver, System
+    build.build()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(args.seed)
+
+    def timed(fn, reps=1):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            out = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps, out
+
+    def emit(d):
+        print(json.dumps({"config_run": True, **d}), flush=True)
+
+    # C2: uniform angles, b = M^dag eta
+    L, Lt = 24, 240
+    N = L * L * Lt
+    boson = torch.tensor(rng.uniform(-np.pi, np.pi, size=(1, 2, L, L, Lt)), device=dev)
+    phi = ref_to_kernel(boson).reshape(1, -1)
+    eta = torch.randn((1, N), dtype=torch.complex128, device=dev) / math.sqrt(2)
+    b = ops.apply_operator("mh", phi, eta, L, 0.1)
+    for prec, rdt, cdt, bps in (("c64", torch.float32, torch.complex64, 24), ("c128", torch.float64,
+                                                                             torch.complex128, 48)):
+        phi_p, b_p = phi.to(rdt), b.to(cdt)
+        out = torch.empty_like(b_p)
+        ms, _ = timed(lambda: ops.apply_operator("mhm", phi_p, b_p, L, 0.1, out=out), reps=20)
+        emit({"config": "C2", "what": f"M^dag M {prec}, 1 rhs (a single launch of 138,240 sites)", "ms": ms,
+              "GBps": bps * N / (ms / 1e3) / 1e9})
+    for mode in ("mixed", "fp64"):
+        s = PcgSolver([System(L, Lt, 1)], mode=mode, rtol=1e-8, max_iter=100000, device=dev)
+        args_ = (phi.reshape(-1).to(s.angle_dtype), b.reshape(-1).to(s.vec_dtype))
+        ms, res = timed(lambda: s.solve(*args_))
+        emit({"config": "C2", "what": f"PCG to 1e-8, {mode}", "ms": ms, "iters": int(res.iters.max()),
+              "relres": float(res.relres.max()), "status": int(res.status.max())})
+
+    # C4a: 64 Z2 noise vectors sharing one L=36 field
+    L, Lt, nrv = 36, 360, 64
+    bos = torch.tensor(pi_flux_np(rng, L, Lt, 1), device=dev)
+    se = StochaticEstimator(L, Lt, Nrv=nrv, precision="mixed", cg_rtol=1e-10, device=dev, seed=5, noise="z2")
+    eta = se.random_vec_bin()
+    ms, _ = timed(lambda: se.set_eta_G_eta(bos, eta))
+    emit({"config": "C4a", "what": "G_eta = (M^dag M)^-1 M^dag eta, 64 rhs, mixed, rtol 1e-10", "ms": ms,
+          "iters": int(se.iters.max()), "relres": float(se.relres.max())})
+
+    # C4b: 16 lattices L in {12, 18, 24, 30} x 4, Ltau = 10 L, one launch
+    Ls = [12, 18, 24, 30] * 4
+    systems = [System(L, 10 * L, 1) for L in Ls]
+    phis = [ref_to_kernel(torch.tensor(pi_flux_np(rng, L, 10 * L, 1), device=dev)).reshape(-1) for L in Ls]
+    rhs = [torch.randn(10 * L ** 3, dtype=torch.complex128, device=dev) / math.sqrt(2) for L in Ls]
+    s = PcgSolver(systems, mode="mixed", rtol=1e-10, max_iter=20000, device=dev)
+    args_ = (torch.cat(phis).float(), torch.cat(rhs))
+    ms, res = timed(lambda: s.solve(*args_))
+    emit({"config": "C4b", "what": "16 uneven lattices, one launch, mixed, rtol 1e-10", "ms": ms,
+          "iters_min": int(res.iters.min()), "iters_max": int(res.iters.max()),
+          "relres_max": float(res.relres.max())})
+
+    # C5: one 30-step trajectory at L=66, Ltau=660 (mixed)
+    L, Lt = 66, 660
+    hmc = HmcSampler(Lx=L, Ltau=Lt, bs=1, precision="mixed", cg_rtol=1e-10, max_iter=50000, delta_t=0.02,
+                     N_leapfrog=30, device=dev, seed=6)
+    b0 = torch.tensor(pi_flux_np(rng, L, Lt, 1), dtype=torch.float32, device=dev)
+    ms, out = timed(lambda: hmc.leapfrog_proposer5(b0))
+    emit({"config": "C5", "what": "one trajectory, 30 leapfrog steps of 0.02, mixed, rtol 1e-10", "ms": ms,
+          "cg_iters_per_solve": float(out[3].float().mean()), "delta_H": float(out[2] - out[1])})
+    return 0
+
+
 def run_matvec_only(args):
     """Three warm-up and ten timed launches of M^dag M on the bench lattice: the
     small, self-contained case that ncu captures of the operator kernel use."""
@@ -574,6 +658,8 @@ def main(argv=None):
         return run_solve_only(args)
     if args.matvec_only > 0:
         return run_matvec_only(args)
+    if args.configs:
+        return run_configs(args)
     return run_native(args)
 
 
