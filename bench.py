@@ -594,6 +594,9 @@ def run_configs(args):
     ms, _ = timed(lambda: se.set_eta_G_eta(bos, eta))
     emit({"config": "C4a", "what": "G_eta = (M^dag M)^-1 M^dag eta, 64 rhs, mixed, rtol 1e-10", "ms": ms,
           "iters": int(se.iters.max()), "relres": float(se.relres.max())})
+    ms, _ = timed(lambda: se.get_bond_bond_per_b2(bos))
+    emit({"config": "C4a", "what": "bond-bond correlators T1+T21+T2+T4+Tvv over the 2016 noise pairs "
+                                   "(complex128, cuFFT)", "ms": ms})
 
     # C4b: 16 lattices L in {12, 18, 24, 30} x 4, Ltau = 10 L, one launch
     Ls = [12, 18, 24, 30] * 4

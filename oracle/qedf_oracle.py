@@ -613,3 +613,102 @@ def g_eta(phi_slice_k, eta, L, cp: Couplings, rtol, max_iter, P_tau=None):
     psi = mh_vec(phi, eta.reshape(nrv, Nt, Vs), L, cp.dtau, cp.t)
     x, it, err = solve_xi(np.ascontiguousarray(phi), psi, L, cp, rtol, max_iter, P_tau)
     return x.reshape(nrv, -1), it, err
+
+
+# ----------------------------------------------------------------------------
+# bond-bond correlators of the stochastic estimator
+# (stochastic_estimator.py T1 :1393, T21 :1447, T2 :1504, T4 :1561, Tvv :1612,
+#  get_bond_bond_per_b2 :2594, bond_corr :2643)
+# ----------------------------------------------------------------------------
+#
+# eta, G_eta: [Nrv, Ltau * L * L] (index tau Vs + x + L y); boson: reference
+# layout [1, 2, Lx, Ly, Ltau].  Each T sums, over the noise pairs s < s'
+# (itertools order) and over tau, the spatial correlation
+#     C(d) = (1 / Vs) sum_r a(r) b(r + d)
+# of two bond products, as the FFT identity ifft(ifft(a) fft(b)) with the
+# reference's norms, and averages; "shift k" is a roll along x by -k (the value
+# at x + k), as torch.roll(..., shifts=-k, dims=-1).
+
+
+def _bb_fields(eta, G, boson, L, Nt):
+    ec = np.conj(eta).reshape(-1, Nt, L, L)
+    g = G.reshape(-1, Nt, L, L)
+    phx = np.transpose(boson, (0, 1, 4, 3, 2))[0, 0]  # [Ltau, Ly, Lx]
+    return ec, g, phx
+
+
+def _sx(a, k):
+    return np.roll(a, -k, axis=-1)
+
+
+def _corr(a, b):
+    aF = np.fft.ifft2(a, norm="backward")
+    bF = np.fft.fft2(b, norm="forward")
+    return np.fft.ifft2(aF * bF, norm="forward")
+
+
+def _pairs(nrv):
+    return [(s, t) for s in range(nrv) for t in range(s + 1, nrv)]
+
+
+def _pair_mean(fa, fb, nrv, L):
+    acc = np.zeros((L, L), dtype=complex)
+    P = _pairs(nrv)
+    for s, t in P:
+        acc += _corr(fa(s, t), fb(s, t)).mean(axis=0)
+    return acc / len(P)
+
+
+def bb_T1(eta, G, boson, L, Nt):
+    ec, g, ph = _bb_fields(eta, G, boson, L, Nt)
+    e = np.exp(1j * ph)
+    out = -_pair_mean(lambda s, t: ec[s] * _sx(g[t], 1) * e, lambda s, t: _sx(g[s], 1) * ec[t] * e, len(ec), L)
+    out[0, -1] += (_sx(g, 1) * np.roll(ec, 1, axis=-1) * e * np.exp(1j * np.roll(ph, 1, axis=-1))).mean()
+    return out
+
+
+def bb_T21(eta, G, boson, L, Nt):
+    ec, g, ph = _bb_fields(eta, G, boson, L, Nt)
+    fa = lambda s, t: (_sx(ec[s], 1) * g[t] + _sx(ec[t], 1) * g[s]) * np.exp(-1j * ph) / 2
+    fb = lambda s, t: (_sx(g[s], 1) * ec[t] + _sx(g[t], 1) * ec[s]) * np.exp(1j * ph) / 2
+    out = -_pair_mean(fa, fb, len(ec), L)
+    out[0, 0] += (g * ec).mean()
+    return out
+
+
+def bb_T2(eta, G, boson, L, Nt):
+    ec, g, ph = _bb_fields(eta, G, boson, L, Nt)
+    fa = lambda s, t: (ec[s] * _sx(g[t], 1) + ec[t] * _sx(g[s], 1)) * np.exp(1j * ph) / 2
+    fb = lambda s, t: (g[s] * _sx(ec[t], 1) + g[t] * _sx(ec[s], 1)) * np.exp(-1j * ph) / 2
+    out = -_pair_mean(fa, fb, len(ec), L)
+    out[0, 0] += (g * ec).mean()
+    return out
+
+
+def bb_T4(eta, G, boson, L, Nt):
+    ec, g, ph = _bb_fields(eta, G, boson, L, Nt)
+    e = np.exp(-1j * ph)
+    out = -_pair_mean(lambda s, t: _sx(ec[s], 1) * g[t] * e, lambda s, t: g[s] * _sx(ec[t], 1) * e, len(ec), L)
+    out[0, 1] += (g * _sx(ec, 2) * e * np.exp(-1j * _sx(ph, 1))).mean()
+    return out
+
+
+def bb_Tvv(eta, G, boson, L, Nt):
+    ec, g, ph = _bb_fields(eta, G, boson, L, Nt)
+    v = _sx(g, 1) * ec * np.exp(1j * ph) + g * _sx(ec, 1) * np.exp(-1j * ph)
+    return _corr(v, v).mean(axis=(0, 1)), v.mean(axis=(0, 1))
+
+
+def bb_observables(eta, G, boson, L, Nt):
+    """get_bond_bond_per_b2: BB0_r, BB_r, B_r, BB_k (real parts, BB_k reordered
+    to ascending momenta)."""
+    T = bb_T1(eta, G, boson, L, Nt) + bb_T21(eta, G, boson, L, Nt) + bb_T2(eta, G, boson, L, Nt) + \
+        bb_T4(eta, G, boson, L, Nt)
+    Tvv, Tv = bb_Tvv(eta, G, boson, L, Nt)
+    BB_r = T * 2 + Tvv * 4
+    BB_k = np.roll(np.fft.ifft2(BB_r, norm="forward"), (L // 2, L // 2), axis=(0, 1))
+    return {"BB0_r": (T * 2).real, "BB_r": BB_r.real, "B_r": Tv.real, "BB_k": BB_k.real}
+
+
+def bb_bond_corr(BB_r_mean, B_r_mean):
+    return BB_r_mean - 4 * _corr(B_r_mean, B_r_mean)

@@ -14,6 +14,7 @@ import torch
 
 from . import ops
 from .hmc import ref_to_kernel
+from .observables import BondBond
 from .solver import PcgSolver, System
 
 
@@ -53,3 +54,31 @@ class StochaticEstimator:
         self.G_eta = res.x.view(self.Nrv, -1)
         self.iters, self.relres, self.status = res.iters, res.relres, res.status
         return self.G_eta
+
+    # ---- bond-bond correlators (reference :1393-1652, :2594-2651) -------------
+    def _bb(self):
+        if getattr(self, "_bond_bond", None) is None:
+            self._bond_bond = BondBond(self.Lx, self.Ltau)
+        return self._bond_bond
+
+    def T1(self, eta, G_eta, boson):
+        return self._bb().T1(eta, G_eta, boson)
+
+    def T21(self, eta, G_eta, boson):
+        return self._bb().T21(eta, G_eta, boson)
+
+    def T2(self, eta, G_eta, boson):
+        return self._bb().T2(eta, G_eta, boson)
+
+    def T4(self, eta, G_eta, boson):
+        return self._bb().T4(eta, G_eta, boson)
+
+    def Tvv(self, eta, G_eta, boson):
+        return self._bb().Tvv(eta, G_eta, boson)
+
+    def get_bond_bond_per_b2(self, boson):
+        """The observables of the current eta / G_eta (after set_eta_G_eta)."""
+        return self._bb().get_bond_bond_per_b2(self.eta, self.G_eta, boson)
+
+    def bond_corr(self, BB_r_mean, B_r_mean):
+        return self._bb().bond_corr(BB_r_mean, B_r_mean)

@@ -2,7 +2,8 @@
 
 Run in a container where the reference source tree is present:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py /root/reference          # golden_ref.npz, golden_traj.npz
+    python tests/golden/make_golden.py /root/reference bond     # golden_bond.npz
 
 The reference module ``qed_fermion.hmc_sampler_batch`` imports ``matplotlib``
 and ``matlab.engine`` at module level; neither is needed for the CPU path, so
@@ -271,5 +272,57 @@ def main():
     print("wrote", sorted(out.keys()) + sorted(traj.keys()))
 
 
+
+
+
+def gen_bond_observables(ref_root, rng):
+    """The reference estimator's bond-bond correlators (stochastic_estimator.py
+    T1 :1393, T21 :1447, T2 :1504, T4 :1561, Tvv :1612, get_bond_bond_per_b2
+    :2594, bond_corr :2643) on L=6, Ltau=12 with 12 noise vectors, G_eta from a
+    dense solve of M in complex128.  The estimator's constructor would load the
+    sampler's preconditioner from the reference's source tree; the correlators do
+    not use it, so a placeholder stands in."""
+    import torch
+    import qed_fermion.hmc_sampler_batch as H
+    import qed_fermion.stochastic_estimator as SE
+    L, Nt, nrv = 6, 12, 12
+    hmc = make_sampler(H, L, Nt)
+    hmc.precon_csr = "unused"
+    b = pi_flux_boson(rng, L, Nt)
+    boson = torch.tensor(b, dtype=torch.float64)
+    _, _, _, M = H.HmcSampler.get_M_sparse(hmc, boson)
+    N = L * L * Nt
+    re = rng.integers(0, 2, size=(nrv, N)) * 2 - 1
+    im = rng.integers(0, 2, size=(nrv, N)) * 2 - 1
+    eta = torch.tensor((re + 1j * im) / math.sqrt(2), dtype=torch.complex128)
+    G = torch.linalg.solve(M.to_dense(), eta.T).T.contiguous()
+    SE.Nrv = nrv
+    se = SE.StochaticEstimator(hmc)
+    se.Nrv = nrv
+    se.initialize()
+    se.eta, se.G_eta = eta, G
+    out = {"bb_boson": b, "bb_eta": eta.numpy(), "bb_G_eta": G.numpy()}
+    for name in ("T1", "T21", "T2", "T4"):
+        out[f"bb_{name}"] = getattr(se, name)(eta, G, boson).numpy()
+    tvv, tv = se.Tvv(eta, G, boson)
+    out["bb_Tvv"], out["bb_Tv"] = tvv.numpy(), tv.numpy()
+    obsr = se.get_bond_bond_per_b2(boson)
+    for k in ("BB0_r", "BB_r", "B_r", "BB_k"):
+        out[f"bb_obsr_{k}"] = obsr[k].numpy()
+    out["bb_bond_corr"] = se.bond_corr(obsr["BB_r"], obsr["B_r"]).numpy()
+    return out
+
+
+def main_bond(ref_root):
+    import_reference(ref_root)
+    rng = np.random.default_rng(20241203)
+    out = gen_bond_observables(ref_root, rng)
+    np.savez_compressed(os.path.join(HERE, "golden_bond.npz"), **out)
+    print("wrote", sorted(out))
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 2 and sys.argv[2] == "bond":
+        main_bond(sys.argv[1])
+    else:
+        main()

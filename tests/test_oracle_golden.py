@@ -166,3 +166,22 @@ def test_trajectory_matches_reference(T):
     dH_ref = T["traj_Hfin"] - T["traj_H0"]
     assert abs((H1 - H0)[0] - dH_ref[0]) < 1e-6 * abs(T["traj_H0"][0])
     np.testing.assert_allclose(x, T["traj_x"], rtol=0, atol=1e-8)
+
+
+def test_bond_bond_correlators_match_reference():
+    """The oracle's T1, T21, T2, T4, Tvv, get_bond_bond_per_b2 and bond_corr
+    against the reference's own (stochastic_estimator.py:1393-1652, 2594-2651)."""
+    G = dict(np.load(os.path.join(HERE, "golden", "golden_bond.npz")))
+    L, Nt = 6, 12
+    args = (G["bb_eta"], G["bb_G_eta"], G["bb_boson"], L, Nt)
+
+    def rel(a, b):
+        return np.abs(a - b).max() / np.abs(b).max()
+    for name, f in (("T1", O.bb_T1), ("T21", O.bb_T21), ("T2", O.bb_T2), ("T4", O.bb_T4)):
+        assert rel(f(*args), G[f"bb_{name}"]) < 1e-12, name
+    tvv, tv = O.bb_Tvv(*args)
+    assert rel(tvv, G["bb_Tvv"]) < 1e-12 and rel(tv, G["bb_Tv"]) < 1e-12
+    ob = O.bb_observables(*args)
+    for k in ("BB0_r", "BB_r", "B_r", "BB_k"):
+        assert rel(ob[k], G[f"bb_obsr_{k}"]) < 1e-12, k
+    assert rel(O.bb_bond_corr(G["bb_obsr_BB_r"], G["bb_obsr_B_r"]), G["bb_bond_corr"]) < 1e-12
