@@ -19,12 +19,14 @@ Precision ("precision" argument):
 """
 from __future__ import annotations
 
+import collections
 import math
 import os
 
 import torch
 
 from . import ops
+from .fourier_mass import FourierMass
 from .solver import PcgSolver, System
 
 PRECISIONS = ("fp64", "mixed", "fp32")
@@ -43,7 +45,8 @@ def kernel_to_ref(phi: torch.Tensor, Lx: int, Ltau: int) -> torch.Tensor:
 class HmcSampler:
     def __init__(self, Lx=6, Ltau=10, J=1.0, K=1.0, dtau=0.1, bs=1, delta_t=0.06, N_leapfrog=5, m=1.0,
                  compact=False, precision="mixed", cg_rtol=1e-10, max_iter=20000, use_precon=True,
-                 ru_interval=50, ru_delta=0.1, device=None, seed=None, solver_impl="persistent"):
+                 ru_interval=50, ru_delta=0.1, device=None, seed=None, solver_impl="persistent",
+                 max_tau_block_idx=1):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}")
         if Lx % 2:
@@ -85,6 +88,15 @@ class HmcSampler:
         self._precon_tau = None
         self.boson = None
         self.last_cg_iters = None
+        # tau-block updates and step-size adaptation (hmc_sampler_batch.py:158-163,
+        # 263-268): blocks only when Ltau >= 10 Lx; per chain a queue of the last
+        # 5 x blocks clipped acceptance probabilities
+        self.tau_block_idx = 0
+        self.max_tau_block_idx = max_tau_block_idx if Ltau // Lx // 10 >= 1 else 1
+        self.tau_block_size = Ltau // self.max_tau_block_idx
+        self.threshold_queue = [collections.deque(maxlen=5 * self.max_tau_block_idx) for _ in range(bs)]
+        self.lower_limit = 0.25
+        self.upper_limit = 0.5
 
     # ---- couplings ---------------------------------------------------------
     @property
@@ -167,6 +179,30 @@ class HmcSampler:
         g = torch.Generator()
         g.manual_seed(int(torch.randint(0, 2 ** 31 - 1, (1,), device=self.device, generator=self.generator).item()))
         return g
+
+    # ---- adaptive Fourier mass (reference :272-285, 1133-1277) -----------------
+    # The reference computes these but its leapfrog does not call the draw or
+    # M^{-1} (the call sites are commented out); they are kept for the API.
+    @property
+    def fourier_mass(self):
+        if getattr(self, "_fourier_mass", None) is None:
+            self._fourier_mass = FourierMass(self.bs, self.Lx, self.Ltau, dtype=self.dtype, device=self.device)
+        return self._fourier_mass
+
+    def update_sigma_hat_cpu(self, boson_cpu, i):
+        self.fourier_mass.update_sigma_hat_cpu(boson_cpu, i)
+
+    def apply_sigma_hat_cpu(self, i):
+        self.fourier_mass.apply_sigma_hat_cpu(i)
+
+    def stabilize_sigma_hat(self, method="shrink", **kw):
+        self.fourier_mass.stabilize_sigma_hat(method, **kw)
+
+    def draw_momentum_fft(self):
+        return self.fourier_mass.draw_momentum_fft(self.generator)
+
+    def apply_m_inv(self, p):
+        return self.fourier_mass.apply_m_inv(p)
 
     # ---- random draws (reference :1247-1252, :1279-1287) ----------------------
     def draw_momentum(self):
@@ -320,11 +356,53 @@ class HmcSampler:
         return (kernel_to_ref(x, Lx, Ltau), H0, H_fin, torch.stack(iters).mean(dim=0),
                 torch.stack(errs).mean(dim=0))
 
-    def metropolis_update(self, tau_mask=None):
-        """One Metropolis step on ``self.boson`` (reference :2886-2930); the
-        accept test ``u < exp(H_old - H_new)`` is evaluated in double."""
+    def _metropolis_step(self, tau_mask):
         boson_new, H_old, H_new, it, err = self.leapfrog_proposer5(self.boson, tau_mask)
         u = torch.rand(self.bs, device=self.device, dtype=torch.float64, generator=self.generator)
         accp = u < torch.exp(H_old - H_new)
         self.boson = torch.where(accp.view(-1, 1, 1, 1, 1), boson_new.to(self.boson.dtype), self.boson)
+        thresholds = torch.clamp(torch.exp(H_old - H_new), max=1.0).cpu().tolist()
+        for b in range(self.bs):
+            self.threshold_queue[b].append(thresholds[b])
+        return accp, it, err, H_old, H_new
+
+    def metropolis_update(self, tau_mask=None):
+        """Metropolis update of ``self.boson`` (reference :2886-2930).  Without
+        ``tau_mask``, one proposal per tau block (``max_tau_block_idx`` blocks of
+        ``tau_block_size`` slices, each moving only its own slices) with its own
+        accept test; with ``tau_mask`` (``[1, 1, 1, 1, Ltau]`` or ``[Ltau]``), one
+        proposal under that mask.  The accept test ``u < exp(H_old - H_new)`` is
+        evaluated in double; every test appends min(exp(H_old - H_new), 1) to the
+        chain's threshold queue.  Returns (boson, accp, iters, err, H_old, H_new)
+        of the last proposal."""
+        if tau_mask is not None:
+            accp, it, err, H_old, H_new = self._metropolis_step(tau_mask)
+            return self.boson, accp, it, err, H_old, H_new
+        if self.max_tau_block_idx == 1:
+            accp, it, err, H_old, H_new = self._metropolis_step(None)
+            return self.boson, accp, it, err, H_old, H_new
+        while self.tau_block_idx < self.max_tau_block_idx:
+            t0 = self.tau_block_idx * self.tau_block_size
+            mask = torch.zeros((1, 1, 1, 1, self.Ltau), device=self.device, dtype=self.dtype)
+            mask[..., t0:t0 + self.tau_block_size] = 1.0
+            accp, it, err, H_old, H_new = self._metropolis_step(mask)
+            self.tau_block_idx += 1
+        self.tau_block_idx = 0
         return self.boson, accp, it, err, H_old, H_new
+
+    def adjust_delta_t(self):
+        """Per chain, once its threshold queue is full: shrink delta_t by 0.9 when
+        the mean clipped acceptance is below ``lower_limit``, grow it by 1.1 when
+        above ``upper_limit``, and clear the queue (reference :699-724)."""
+        for b in range(self.bs):
+            q = self.threshold_queue[b]
+            if len(q) < q.maxlen:
+                continue
+            rate = sum(q) / len(q)
+            if rate < self.lower_limit:
+                self.delta_t_tensor[b] *= 0.9
+            elif self.upper_limit < rate:
+                self.delta_t_tensor[b] *= 1.1
+            else:
+                continue
+            q.clear()

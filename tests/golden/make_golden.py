@@ -4,6 +4,7 @@ Run in a container where the reference source tree is present:
 
     python tests/golden/make_golden.py /root/reference          # golden_ref.npz, golden_traj.npz
     python tests/golden/make_golden.py /root/reference bond     # golden_bond.npz
+    python tests/golden/make_golden.py /root/reference fourier  # golden_fourier_mass.npz
 
 The reference module ``qed_fermion.hmc_sampler_batch`` imports ``matplotlib``
 and ``matlab.engine`` at module level; neither is needed for the CPU path, so
@@ -321,8 +322,48 @@ def main_bond(ref_root):
     print("wrote", sorted(out))
 
 
+def gen_fourier_mass(rng):
+    """The reference's adaptive Fourier mass (hmc_sampler_batch.py:272-285,
+    1133-1277) on L=4, Ltau=10: 12 fields folded into the statistics with a
+    window of 5 and annealing every 4 steps, the mass formed at step 10 in mass
+    modes 1 and -1, M^{-1} applied to a momentum, and a momentum drawn with a
+    seeded torch generator."""
+    import torch
+    import qed_fermion.hmc_sampler_batch as H
+    out = {}
+    L, Nt = 4, 10
+    fields = rng.standard_normal((12, 1, 2, L, L, Nt))
+    p = rng.standard_normal((1, 2, L, L, Nt))
+    out["fm_fields"], out["fm_p"] = fields, p
+    for mode in (1, -1):
+        H.mass_mode = mode
+        hmc = make_sampler(H, L, Nt)
+        hmc.sigma_mini_batch_size = 5
+        hmc.annealing_step = 4
+        for i in range(12):
+            hmc.update_sigma_hat_cpu(torch.tensor(fields[i]), i)
+        out[f"fm{mode}_sigma_hat_cpu"] = hmc.sigma_hat_cpu.numpy()
+        out[f"fm{mode}_boson_mean_cpu"] = hmc.boson_mean_cpu.numpy()
+        hmc.apply_sigma_hat_cpu(10)
+        out[f"fm{mode}_sigma_hat"] = hmc.sigma_hat.numpy()
+        out[f"fm{mode}_m_inv_p"] = hmc.apply_m_inv(torch.tensor(p)).numpy()
+        torch.manual_seed(77)
+        out[f"fm{mode}_p_fft"] = hmc.draw_momentum_fft().numpy()
+    H.mass_mode = 0
+    return out
+
+
+def main_fourier(ref_root):
+    import_reference(ref_root)
+    out = gen_fourier_mass(np.random.default_rng(20241204))
+    np.savez_compressed(os.path.join(HERE, "golden_fourier_mass.npz"), **out)
+    print("wrote", sorted(out))
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 2 and sys.argv[2] == "bond":
         main_bond(sys.argv[1])
+    elif len(sys.argv) > 2 and sys.argv[2] == "fourier":
+        main_fourier(sys.argv[1])
     else:
         main()
