@@ -38,6 +38,9 @@ UNIT = "trajectories/hour"
 # dram__bytes_read.sum,dram__bytes_write.sum of `bench.py --solve-only 482`
 # (profiles/k_pcg_mixed_L48_Lt480_rhs2.md)
 PCG_DRAM_BYTES_PER_SITE_ITER = 71.1
+# PCG iterations per solve of this workload (mixed, rtol 1e-10), as the GPU run
+# measures them; the CPU arms extrapolate a trajectory with it when they run alone
+CG_ITERS_PER_SOLVE = 482
 
 
 def parse_args(argv=None):
@@ -135,43 +138,23 @@ class ClockSampler:
 # reference arm / CPU baseline: the oracle (CPU restatement of the reference)
 # ---------------------------------------------------------------------------
 def cpu_sample(L, Ltau, seed, seconds):
-    """Time the CPU restatement on the same lattice: PCG iterations (M^dag M,
-    preconditioner, axpys, dots) and one fermion force.  Returns per-unit
-    seconds and what was sampled."""
+    """Time the CPU restatement of the path on all host cores (the C/OpenMP port
+    of the oracle, oracle/qedf_cpu.c) on the same lattice and start: PCG
+    iterations (M^dag M, preconditioner, axpys, dots) and fermion forces.
+    Returns per-unit seconds, what was sampled and the thread count."""
     import numpy as np
+    from oracle import cpu_port as C
     from oracle import qedf_oracle as O
+    C.build()
     rng = np.random.default_rng(seed)
     Vs = L * L
-    boson = pi_flux_np(rng, L, Ltau, 1)
-    phi = O.ref_to_kernel_layout(boson)
-    v = (rng.standard_normal((1, Ltau, Vs)) + 1j * rng.standard_normal((1, Ltau, Vs))) / math.sqrt(2)
-    P = O.precon_tau_matrix(Ltau) if Ltau >= O.precon_min_ltau() else None
-    t0 = time.perf_counter()
-    n_it = 0
-    x = np.zeros_like(v)
-    r = v.copy()
-    p = r.copy()
-    while True:
-        Op = O.mhm_vec(phi, p, L, 0.1)
-        a = np.vdot(r, r).real / np.vdot(p, Op).real
-        x = x + a * p
-        r = r - a * Op
-        z = O.precon_vec(r, P) if P is not None else r
-        b = np.vdot(r, z).real
-        p = z + 0.5 * p
-        n_it += 1
-        if time.perf_counter() - t0 > seconds * 0.6 and n_it >= 1:
-            break
-    t_it = (time.perf_counter() - t0) / n_it
-    t1 = time.perf_counter()
-    n_f = 0
-    while True:
-        O.force_f_from_xi(phi, v, L, 0.1)
-        n_f += 1
-        if time.perf_counter() - t1 > seconds * 0.3:
-            break
-    t_force = (time.perf_counter() - t1) / n_f
-    return t_it, t_force, f"{n_it} PCG iterations + {n_f} fermion forces of the numpy oracle at L={L}, Ltau={Ltau}"
+    phi = O.ref_to_kernel_layout(pi_flux_np(rng, L, Ltau, 1))[0]
+    v = (rng.standard_normal((Ltau, Vs)) + 1j * rng.standard_normal((Ltau, Vs))) / math.sqrt(2)
+    csr = C.csr_of(O.precon_tau_matrix(Ltau)) if Ltau >= O.precon_min_ltau() else None
+    t_it, t_force, n_it, n_f = C.time_sample(phi, v, L, 0.1, csr, seconds)
+    nth = C.threads()
+    return t_it, t_force, (f"{n_it} PCG iterations + {n_f} fermion forces of the C/OpenMP port of the oracle "
+                           f"(complex128) at L={L}, Ltau={Ltau} on {nth} threads"), nth
 
 
 def cpu_traj_per_hour(t_it, t_force, iters_per_solve, n_leapfrog):
@@ -186,20 +169,20 @@ def run_reference(args):
         return 0
     iters = args.cg_iters_per_solve
     if iters is None:
-        iters = float(os.environ.get("QEDF_CG_ITERS_PER_SOLVE", "250"))
+        iters = float(os.environ.get("QEDF_CG_ITERS_PER_SOLVE", CG_ITERS_PER_SOLVE))
     per_step = []
-    sample = ""
+    sample, nth = "", 1
     for k in range(args.warmup + args.steps):
-        t_it, t_force, sample = cpu_sample(args.L, args.Ltau, args.seed + k, args.cpu_seconds / 2)
+        t_it, t_force, sample, nth = cpu_sample(args.L, args.Ltau, args.seed + k, args.cpu_seconds / 2)
         if k >= args.warmup:
             per_step.append(cpu_traj_per_hour(t_it, t_force, iters, args.n_leapfrog))
     value = statistics.median(per_step)
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3600e3 / value,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64 (numpy)",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64 (C/OpenMP)",
         "data": "synthetic", "config": workload_config(args),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port",
                          "sample": sample + f"; extrapolated with {iters:g} PCG iterations per solve, "
                                             f"{args.n_leapfrog + 1} solves + forces per trajectory"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -468,9 +451,9 @@ def run_native(args):
     # --- CPU baseline (oracle restatement) on a bounded sample
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0 and not args.quick:
-        t_it, t_force, sample = cpu_sample(L, Lt, seed, args.cpu_seconds)
-        ips = result.get("cg_iters_per_solve") or 250
-        cpu = {"value": cpu_traj_per_hour(t_it, t_force, ips, args.n_leapfrog), "unit": UNIT, "cores": 1,
+        t_it, t_force, sample, nth = cpu_sample(L, Lt, seed, args.cpu_seconds)
+        ips = result.get("cg_iters_per_solve") or CG_ITERS_PER_SOLVE
+        cpu = {"value": cpu_traj_per_hour(t_it, t_force, ips, args.n_leapfrog), "unit": UNIT, "cores": nth,
                "kind": "port", "sample": sample + f"; extrapolated with the {ips:.0f} PCG iterations per solve "
                                                   f"this run needed, {args.n_leapfrog + 1} solves per trajectory",
                "s_per_cg_iteration": t_it, "s_per_force": t_force}
