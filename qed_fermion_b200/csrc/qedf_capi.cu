@@ -38,8 +38,7 @@ int op_entry(int op, const A* boson, const R* x, R* out, int bs, int Lx, int Lta
   a.bs = bs;
   a.rhs_per_phi = rhs_per_boson;
   a.T = slab;
-  a.xs = std::getenv("QEDF_NO_XS") ? 0 : 1;  // tuning switch: warp-shuffle engine off
-  a.variant = std::getenv("QEDF_VARIANT") ? std::atoi(std::getenv("QEDF_VARIANT")) : 0;
+  a.xs = 1;
   a.c1 = f.c1;
   a.ch = f.ch;
   a.t1 = f.t1;
@@ -178,7 +177,6 @@ int pcg_solve_ws(const qedf_system* sys, int nsys, const void* boson, const void
   PcgParams p;
   int e = pcg_plan(p, sys, nsys, opts);
   if (e) return e;
-  p.variant = std::getenv("QEDF_VARIANT") ? std::atoi(std::getenv("QEDF_VARIANT")) : 0;
   if (!boson || !b || !x || !iters || !relres || !status || !workspace) return QEDF_ERR_ARG;
   if (!aligned16(boson) || !aligned16(b) || !aligned16(x) || !aligned16(workspace)) return QEDF_ERR_ARG;
   if (opts->max_iter < 0 || !(opts->rtol >= 0)) return QEDF_ERR_ARG;

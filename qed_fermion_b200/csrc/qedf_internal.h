@@ -18,7 +18,6 @@ struct OpArgs {
   int rhs_per_phi;  // consecutive vectors sharing one angle array
   int T;            // slab length (0 = auto)
   int xs;           // allow the warp-shuffle engine (single precision, L <= 64)
-  int variant;      // 1: phases in shared memory, two blocks per SM (single precision)
   double c1, ch, t1, th, Cb;
 };
 
@@ -110,7 +109,6 @@ struct PcgParams {
   PcgSys sys[PCG_MAX_SYS];
   int mode;  // QEDF_PCG_PLAIN_F32, QEDF_PCG_PLAIN_F64, QEDF_PCG_MIXED
   int xs;    // allow the warp-shuffle engine for the single-precision iterations
-  int variant;  // 1: single-precision engine with phases in shared memory, two blocks per SM
   int max_iter, ru_interval;
   double rtol, ru_delta;
   double c1, ch, t1, th, Cb;

@@ -596,8 +596,6 @@ template <typename R, typename A, int BY>
 static int launch_operator_by(int op, const OpArgs& a, int xs, cudaStream_t st) {
   if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
     return launch_operator_fl<R, A, BY, EC_PHS>(op, a, st);
-  if (sizeof(R) == 4 && a.variant == 1 && 2 * slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
-    return launch_operator_t<R, A, BY, EC_PHS | EC_2CTA>(op, a, st);
   if (sizeof(R) == 4 && xs && xs_possible(a.L) && ((a.L / 2) & (a.L / 2 - 1)) == 0 &&
       slice_threads(a.L, BY, true) <= MaxT<BY, EC_XS>::value)
     return launch_operator_t<R, A, BY, EC_XS>(op, a, st);

@@ -949,14 +949,8 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
   bool pow2 = true;
   for (int s = 0; s < p.nsys; ++s) pow2 = pow2 && (((p.sys[s].L / 2) & (p.sys[s].L / 2 - 1)) == 0);
   const bool xs = p.xs && pow2 && xs_possible(Lmax) && slice_threads(Lmax, BY, true) <= MaxT<BY, EC_XS>::value;
-  int Ntmax = 0;
-  for (int s = 0; s < p.nsys; ++s) Ntmax = std::max(Ntmax, p.sys[s].Nt);
-  const size_t ew = sizeof(float) * 2 * (size_t)Ntmax * PCG_CHUNK;
-  const bool two = p.variant == 1 &&
-                   2 * (std::max(slice_smem_bytes<float, EC_PHS>(Lmax, BY, 2), ew) + sizeof(RhsState)) <= 227 * 1024;
   switch (p.mode) {
     case QEDF_PCG_PLAIN_F32:
-      if (two) return launch_pcg_t<float, float, float, BY, EC_PHS | EC_2CTA, EC_PHS | EC_2CTA>(p, st);
       if (xs && fits(slice_smem_bytes<float, 0>(Lmax, BY, 2)))
         return launch_pcg_t<float, float, float, BY, EC_XS, EC_XS>(p, st);
       if (fits(slice_smem_bytes<float, 0>(Lmax, BY, 2)))
@@ -969,8 +963,6 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
         return launch_pcg_t<double, double, double, BY, 0, 0>(p, st);
       return launch_pcg_t<double, double, double, BY, EC_NOSTASH, EC_NOSTASH>(p, st);
     case QEDF_PCG_MIXED:
-      if (two && 2 * (slice_smem_bytes<double, EC_NOSTASH>(Lmax, BY, 2) + sizeof(RhsState)) <= 227 * 1024)
-        return launch_pcg_t<float, double, float, BY, EC_PHS | EC_2CTA, EC_NOSTASH | EC_2CTA>(p, st);
       if (xs && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
         return launch_pcg_t<float, double, float, BY, EC_XS, EC_PHS>(p, st);
       if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))

@@ -48,10 +48,9 @@ struct MaxThreads {
 //   EC_XS      exchanges of the x-bond factors by warp shuffles: a warp holds
 //              whole rows of tiles (L/2 <= 32 tiles per row, padded to a power
 //              of two), so only the y-bond factors need a block barrier
-//   EC_2CTA    compiled for two resident blocks per SM (register budget halved)
 //   EC_L(l)    (bits 8 and up) the lattice side fixed at compile time, so the
 //              engine's index arithmetic folds into constants; 0 = run-time L
-enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_2CTA = 8 };
+enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4 };
 __host__ __device__ constexpr int EC_L(int l) { return l << 8; }
 __host__ __device__ constexpr int ec_fixed_l(int ec) { return ec >> 8; }
 // the lattice side of a kernel compiled for engine configuration EC
@@ -66,7 +65,7 @@ template <int BY, int EC>
 struct MaxT {
   static constexpr int value = (EC & EC_XS) ? (BY == 2 ? 768 : (BY == 4 ? 512 : 384))
                                             : (BY == 2 ? 576 : (BY == 4 ? 512 : 384));
-  static constexpr int min_blocks = (EC & EC_2CTA) ? 2 : 1;
+  static constexpr int min_blocks = 1;
 };
 
 // threads of one slice engine (a multiple of 32)
