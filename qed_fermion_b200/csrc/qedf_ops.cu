@@ -585,8 +585,10 @@ static int launch_operator_t(int op, const OpArgs& a, cudaStream_t st) {
 // L = 48); every other L runs the run-time-L engine.
 template <typename R, typename A, int BY, int EC>
 static int launch_operator_fl(int op, const OpArgs& a, cudaStream_t st) {
-  if constexpr (BY == 2 && (EC == 0 || EC == EC_PHS))
-    if (a.L == 48) return launch_operator_t<R, A, BY, EC | EC_L(48)>(op, a, st);
+  if constexpr (EC == 0 || EC == EC_PHS)
+    return with_fixed_l<BY>(a.L, [&](auto lt) {
+      return launch_operator_t<R, A, BY, EC | EC_L(decltype(lt)::value)>(op, a, st);
+    });
   return launch_operator_t<R, A, BY, EC>(op, a, st);
 }
 
@@ -672,13 +674,10 @@ static int launch_force_t(const ForceArgs& a, cudaStream_t st) {
 
 template <typename R, typename A, int BY>
 static int launch_force_by(const ForceArgs& a, cudaStream_t st) {
-  // the benchmark lattice L = 48 runs an engine compiled for it
-  if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS | EC_NOSTASH>(a.L, BY, 4) <= smem_limit()) {
-    if (BY == 2 && a.L == 48) return launch_force_t<R, A, BY, true, 48>(a, st);
-    return launch_force_t<R, A, BY, true>(a, st);
-  }
-  if (BY == 2 && a.L == 48) return launch_force_t<R, A, BY, false, 48>(a, st);
-  return launch_force_t<R, A, BY, false>(a, st);
+  // the benchmark lattices run engines compiled for their size
+  if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS | EC_NOSTASH>(a.L, BY, 4) <= smem_limit())
+    return with_fixed_l<BY>(a.L, [&](auto lt) { return launch_force_t<R, A, BY, true, decltype(lt)::value>(a, st); });
+  return with_fixed_l<BY>(a.L, [&](auto lt) { return launch_force_t<R, A, BY, false, decltype(lt)::value>(a, st); });
 }
 
 template <typename R, typename A>

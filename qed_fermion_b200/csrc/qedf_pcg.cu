@@ -930,15 +930,17 @@ int launch_pcg_prep(const PcgParams& p, int zero_words, cudaStream_t st) {
 
 static bool fits(size_t engine_bytes) { return engine_bytes + sizeof(RhsState) <= 227 * 1024; }
 
-// Engines compiled for a fixed lattice side (the benchmark lattice, L = 48)
-// when every system has it; otherwise the run-time-L engine.
+// Engines compiled for a fixed lattice side (with_fixed_l) when every system
+// has that side; otherwise the run-time-L engine.
 template <typename RS, typename RH, typename A, int BY, int ECS, int ECH>
 static int launch_pcg_fl(PcgParams& p, cudaStream_t st) {
-  bool all48 = BY == 2;
-  for (int s = 0; s < p.nsys; ++s) all48 = all48 && p.sys[s].L == 48;
-  if constexpr (BY == 2)
-    if (all48) return launch_pcg_t<RS, RH, A, BY, ECS | EC_L(48), ECH | EC_L(48)>(p, st);
-  return launch_pcg_t<RS, RH, A, BY, ECS, ECH>(p, st);
+  bool same = true;
+  for (int s = 1; s < p.nsys; ++s) same = same && p.sys[s].L == p.sys[0].L;
+  if (!same) return launch_pcg_t<RS, RH, A, BY, ECS, ECH>(p, st);
+  return with_fixed_l<BY>(p.sys[0].L, [&](auto lt) {
+    constexpr int LT = decltype(lt)::value;
+    return launch_pcg_t<RS, RH, A, BY, ECS | EC_L(LT), ECH | EC_L(LT)>(p, st);
+  });
 }
 
 template <int BY>
@@ -960,7 +962,7 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
       if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
         return launch_pcg_fl<double, double, double, BY, EC_PHS, EC_PHS>(p, st);
       if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
-        return launch_pcg_t<double, double, double, BY, 0, 0>(p, st);
+        return launch_pcg_fl<double, double, double, BY, 0, 0>(p, st);
       return launch_pcg_t<double, double, double, BY, EC_NOSTASH, EC_NOSTASH>(p, st);
     case QEDF_PCG_MIXED:
       if (xs && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
@@ -968,7 +970,7 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
       if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
         return launch_pcg_fl<float, double, float, BY, 0, EC_PHS>(p, st);
       if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
-        return launch_pcg_t<float, double, float, BY, 0, 0>(p, st);
+        return launch_pcg_fl<float, double, float, BY, 0, 0>(p, st);
       return launch_pcg_t<float, double, float, BY, 0, EC_NOSTASH>(p, st);
   }
   return QEDF_ERR_ARG;

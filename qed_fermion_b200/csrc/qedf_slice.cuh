@@ -27,6 +27,8 @@
 // the ends of a tile row), and a neighbour's value sits at the neighbour's id.
 #pragma once
 
+#include <type_traits>
+
 #include "qedf_common.cuh"
 
 namespace qedf {
@@ -53,6 +55,21 @@ struct MaxThreads {
 enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4 };
 __host__ __device__ constexpr int EC_L(int l) { return l << 8; }
 __host__ __device__ constexpr int ec_fixed_l(int ec) { return ec >> 8; }
+// Lattice sides with engines compiled for their size: the benchmark
+// configurations' lattices with 2 x 2 tiles (L = 24, 36, 48; measured 2 to 16 %
+// faster per PCG iteration than the run-time-L engine; at L = 66 the 2 x 6 tile
+// engine gained nothing).  Calls f(std::integral_constant<int, LT>) with the
+// side when it is one of them, else with 0 (the run-time-L engine).
+template <int BY, typename F>
+inline int with_fixed_l(int L, F&& f) {
+  if constexpr (BY == 2) {
+    if (L == 48) return f(std::integral_constant<int, 48>{});
+    if (L == 36) return f(std::integral_constant<int, 36>{});
+    if (L == 24) return f(std::integral_constant<int, 24>{});
+  }
+  return f(std::integral_constant<int, 0>{});
+}
+
 // the lattice side of a kernel compiled for engine configuration EC
 template <int EC>
 __host__ __device__ __forceinline__ int lattice_l(int runtime_l) {
