@@ -63,6 +63,8 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--solve-only", type=int, default=0,
                     help="profiling mode: one PCG solve of the workload with exactly this many iterations")
+    ap.add_argument("--kernels", action="store_true",
+                    help="time every library kernel once on the bench lattice, one JSON line each")
     ap.add_argument("--configs", action="store_true",
                     help="time the other benchmark configurations (C2, C4a, C4b, C5), one JSON line each")
     ap.add_argument("--matvec-only", type=int, default=0,
@@ -519,6 +521,85 @@ def run_solve_only(args):
     return 0
 
 
+def run_kernels(args):
+    """Every kernel of the library on L=48, Ltau=480 (2 right-hand sides, each
+    with its own field), after warm-up, timed with CUDA events over 10 launches:
+    the algorithmic bytes of one launch and the bandwidth they imply."""
+    import numpy as np
+    import torch
+    from qed_fermion_b200 import build, ops, precon
+    from qed_fermion_b200.hmc import ref_to_kernel
+    from qed_fermion_b200.solver import PcgSolver, System
+    build.build()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(args.seed)
+    L, Lt, bs = args.L, args.Ltau, 2
+    N = L * L * Lt
+    boson = torch.tensor(pi_flux_np(rng, L, Lt, bs), device=dev)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+
+    def timed(fn, reps=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def emit(kernel, what, ms, nbytes):
+        gbs = nbytes / (ms / 1e3) / 1e9
+        print(json.dumps({"kernel_run": True, "kernel": kernel, "what": what, "ms": ms, "algorithmic_bytes": nbytes,
+                          "GBps": gbs, "frac_of_measured_hbm": gbs / hbm}), flush=True)
+
+    for prec, rdt, cdt, sv, sp in (("c64", torch.float32, torch.complex64, 8, 4),
+                                   ("c128", torch.float64, torch.complex128, 16, 8)):
+        phi = ref_to_kernel(boson).reshape(bs, -1).to(rdt)
+        x = torch.randn((bs, N), dtype=cdt, device=dev)
+        out = torch.empty_like(x)
+        for op in ("m", "mh", "mhm"):
+            ms = timed(lambda: ops.apply_operator(op, phi, x, L, 0.1, out=out))
+            emit(f"k_operator ({op}, {prec})", f"{bs} rhs", ms, bs * N * (2 * sv + 2 * sp))
+        vt = x[:, :L * L].contiguous()
+        ms = timed(lambda: ops.b_vec_per_tau(phi[0, :2 * L * L].contiguous(), vt, L, 0.1, True))
+        emit(f"k_bvec ({prec})", f"{bs} vectors of one slice, six partial products", ms,
+             bs * L * L * (sv + 6 * sv) + 2 * L * L * sp)
+        F = None
+        ms = timed(lambda: ops.fermion_force(phi, x, L, 0.1))
+        emit(f"k_force ({prec})", f"{bs} rhs", ms, bs * N * (sv + 4 * sp))
+        csr = precon.to_device(precon.builtin_tau_csr(Lt), dev)
+        ms = timed(lambda: ops.precon_apply(x, csr, L))
+        emit(f"k_precon ({prec})", f"{bs} rhs", ms, bs * N * 2 * sv)
+        ms = timed(lambda: ops.cdot(x, out))
+        emit(f"k_cdot ({prec})", f"{bs} rows", ms, bs * N * 2 * sv)
+        ang = phi.clone()
+        ms = timed(lambda: ops.boson_force(ang, L, 0.1, 10.0))
+        emit(f"k_boson_force ({prec})", f"{bs} fields", ms, bs * N * 2 * sp * 2)
+        ms = timed(lambda: ops.boson_action(ang, L, 0.1, 10.0, momenta=ang))
+        emit(f"k_boson_action ({prec})", f"{bs} fields with momenta", ms, bs * N * 2 * sp * 2)
+        pm = torch.zeros_like(ang)
+        fm = torch.ones_like(ang)
+        dt = torch.full((bs,), 0.01, dtype=torch.float64, device=dev)
+        ms = timed(lambda: ops.kick_drift(pm, fm, ang, dt, None, 0.5, 1.0, L))
+        emit(f"k_kick_drift ({prec})", f"{bs} fields, kick and drift", ms, bs * N * 2 * sp * 5)
+    for mode in ("mixed", "fp64"):
+        s = PcgSolver([System(L, Lt, bs)], mode=mode, rtol=0.0, max_iter=100, device=dev)
+        a_ = ref_to_kernel(boson).reshape(-1).to(s.angle_dtype)
+        b_ = torch.randn(bs * N, dtype=torch.complex128, device=dev).to(s.vec_dtype)
+        ms = timed(lambda: s.solve(a_, b_), reps=2)
+        sv = 8 if mode == "mixed" else 16
+        emit(f"k_pcg ({mode})", f"100 iterations, {bs} rhs", ms, 100 * bs * N * (7 * sv + 2 * (sv // 2)))
+    return 0
+
+
 def run_configs(args):
     """The benchmark's other configurations on one GPU, each after a warm-up
     run and timed with CUDA events: C2 (L=24 matvec and PCG to 1e-8 in both
@@ -646,6 +727,8 @@ def main(argv=None):
         return run_matvec_only(args)
     if args.configs:
         return run_configs(args)
+    if args.kernels:
+        return run_kernels(args)
     return run_native(args)
 
 
