@@ -171,12 +171,135 @@ __global__ void k_precon(PreconArgs p) {
     Cx<R> acc0 = mk<R>(0, 0), acc1 = mk<R>(0, 0);
     for (int k = p.row_ptr[t]; k < p.row_ptr[t + 1]; ++k) {
       const R w = (R)p.val[k];
+      if ((unsigned)p.col[k] >= (unsigned)p.Nt) continue;  // outside the matrix
       Cx<R> a, b;
       ld2(r + p.col[k] * sv + 2 * s, a, b);
       acc0 = mk<R>(fma(w, a.re, acc0.re), fma(w, a.im, acc0.im));
       acc1 = mk<R>(fma(w, b.re, acc1.re), fma(w, b.im, acc1.im));
     }
     st2(z + t * sv + 2 * s, acc0, acc1);
+  }
+}
+
+// The same product, one block per (128-byte column of sites, right-hand side):
+// 16 complex64 or 8 complex128 sites, 8 threads of 16 bytes per row.  The
+// column's r rows are read once, coalesced, into shared memory.  Each thread
+// then forms C consecutive output rows of its 16 bytes.  Where every one of
+// those rows is the middle CSR row (t = Ltau/2) shifted along tau - taps
+// t-H .. t+H with the same values, as in the bulk of a banded P_tau - a
+// window of 2H+1 rows slides through registers with the taps as constants,
+// one shared-memory row read per output row; other rows run over their CSR
+// row.  Both orders of summation are the CSR order, so the two forms agree
+// bit for bit.
+template <typename R>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  using T = float4;
+  __device__ static T zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+  __device__ static T fma(float c, T q, T a) {
+    return make_float4(fmaf(c, q.x, a.x), fmaf(c, q.y, a.y), fmaf(c, q.z, a.z), fmaf(c, q.w, a.w));
+  }
+};
+template <>
+struct Vec16<double> {
+  using T = double2;
+  __device__ static T zero() { return make_double2(0., 0.); }
+  __device__ static T fma(double c, T q, T a) { return make_double2(::fma(c, q.x, a.x), ::fma(c, q.y, a.y)); }
+};
+
+constexpr int PRE_H = 6;  // half-width of the banded form (13 taps, the builtin P_tau)
+constexpr int PRE_ROW_THREADS = 8;
+
+inline size_t precon_band_smem(int Nt) { return (size_t)Nt * (16 * PRE_ROW_THREADS + 1); }
+
+template <typename R, int H, int C>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_precon_band(PreconArgs p) {
+  using VT = Vec16<R>;
+  using V = typename VT::T;
+  constexpr int PER = 16 / sizeof(Cx<R>);  // complex numbers per thread
+  constexpr int W = PRE_ROW_THREADS * PER;  // sites per column
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int Vs = p.L * p.L, Nt = p.Nt;
+  V* colv = reinterpret_cast<V*>(smem_raw);                                    // [Nt][8]
+  unsigned char* regular = smem_raw + sizeof(V) * PRE_ROW_THREADS * (size_t)Nt;  // [Nt]
+  const int c0 = blockIdx.x * W;
+  const size_t sv = 2 * (size_t)Vs;
+  const R* r = reinterpret_cast<const R*>(p.r) + (size_t)blockIdx.y * Nt * sv + 2 * (size_t)c0;
+  R* z = reinterpret_cast<R*>(p.z) + (size_t)blockIdx.y * Nt * sv + 2 * (size_t)c0;
+  const int j = threadIdx.x % PRE_ROW_THREADS, grp = threadIdx.x / PRE_ROW_THREADS;
+  const int ngrp = blockDim.x / PRE_ROW_THREADS;  // at most 32 chunks
+  const bool jon = j * PER < Vs - c0;
+  __shared__ unsigned irregular_chunks;
+  if (threadIdx.x == 0) irregular_chunks = 0;
+  // the column's rows stream into shared memory while the rows' form is found
+  if (jon)
+    for (int t = grp; t < Nt; t += ngrp)
+      cp_async16(colv + t * PRE_ROW_THREADS + j, reinterpret_cast<const V*>(r + t * sv) + j);
+  cp_async_commit();
+  // which rows are the middle row shifted (independent loads, no early exit)
+  const int tm = Nt / 2, km = p.row_ptr[tm];
+  bool band = Nt > 2 * H && p.row_ptr[tm + 1] - km == 2 * H + 1;
+  double vm[2 * H + 1];
+  if (band) {
+#pragma unroll
+    for (int i = 0; i <= 2 * H; ++i) {
+      vm[i] = p.val[km + i];
+      band &= p.col[km + i] == tm - H + i;
+    }
+  }
+  for (int t = threadIdx.x; t < Nt; t += blockDim.x) {
+    const int k0 = p.row_ptr[t];
+    bool ok = band && t >= H && t < Nt - H && p.row_ptr[t + 1] - k0 == 2 * H + 1;
+    if (ok) {
+#pragma unroll
+      for (int i = 0; i <= 2 * H; ++i) ok &= (p.col[k0 + i] == t - H + i) & (p.val[k0 + i] == vm[i]);
+    }
+    regular[t] = ok;
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  // chunk grp (rows t0 .. t0+C-1) is regular when all its rows are
+  const int t0 = grp * C;
+  bool reg = t0 + C <= Nt;
+  for (int i = 0; reg && i < C; ++i) reg = regular[t0 + i];
+  if (!reg && j == 0) atomicOr(&irregular_chunks, 1u << grp);
+  __syncthreads();
+  if (!jon) return;
+  if (reg) {
+    R c[2 * H + 1];
+#pragma unroll
+    for (int k = 0; k <= 2 * H; ++k) c[k] = (R)vm[k];
+    V w[2 * H + 1];
+#pragma unroll
+    for (int k = 0; k < 2 * H; ++k) w[k + 1] = colv[(t0 - H + k) * PRE_ROW_THREADS + j];
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+#pragma unroll
+      for (int k = 0; k < 2 * H; ++k) w[k] = w[k + 1];
+      w[2 * H] = colv[(t0 + i + H) * PRE_ROW_THREADS + j];
+      V acc = VT::zero();
+#pragma unroll
+      for (int k = 0; k <= 2 * H; ++k) acc = VT::fma(c[k], w[k], acc);
+      __stcg(reinterpret_cast<V*>(z + (t0 + i) * sv) + j, acc);
+    }
+  }
+  // the rows of irregular chunks, spread over all row groups
+  const unsigned mask = irregular_chunks;
+  const int G = __popc(mask) * C;
+  for (int g = grp; g < G; g += ngrp) {
+    unsigned m = mask;
+    for (int q = 0; q < g / C; ++q) m &= m - 1;  // drop the chunks before the (g / C)-th
+    const int t = (__ffs(m) - 1) * C + g % C;
+    if (t >= Nt) continue;
+    V acc = VT::zero();
+    const int k1 = p.row_ptr[t + 1];
+#pragma unroll 4
+    for (int k = p.row_ptr[t]; k < k1; ++k) {
+      const int cc = p.col[k];
+      if ((unsigned)cc < (unsigned)Nt) acc = VT::fma((R)p.val[k], colv[cc * PRE_ROW_THREADS + j], acc);
+    }
+    __stcg(reinterpret_cast<V*>(z + t * sv) + j, acc);
   }
 }
 
@@ -407,20 +530,85 @@ __device__ __forceinline__ void boson_force_site(const A* phi, int L, int Nt, in
 }
 
 template <typename A>
+// grid (site blocks, slice, chain): one site per thread, both bond directions
 __global__ void k_boson_force(BosonArgs p) {
   const int Vs = p.L * p.L;
-  const size_t n = (size_t)p.bs * p.Nt * Vs;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int s = i % Vs;
-    const size_t bt = i / Vs;
-    const int t = bt % p.Nt;
-    const int b = bt / p.Nt;
-    const A* phi = reinterpret_cast<const A*>(p.x) + (size_t)b * p.Nt * 2 * Vs;
-    A fx, fy;
-    boson_force_site<A>(phi, p.L, p.Nt, t, s % p.L, s / p.L, (A)p.K, (A)p.ctau, p.compact, fx, fy);
-    A* F = reinterpret_cast<A*>(p.F) + 2 * i;
-    F[0] = fx;
-    F[1] = fy;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= Vs) return;
+  const int t = blockIdx.y, b = blockIdx.z;
+  const A* phi = reinterpret_cast<const A*>(p.x) + (size_t)b * p.Nt * 2 * Vs;
+  A fx, fy;
+  boson_force_site<A>(phi, p.L, p.Nt, t, s % p.L, s / p.L, (A)p.K, (A)p.ctau, p.compact, fx, fy);
+  A* F = reinterpret_cast<A*>(p.F) + 2 * (((size_t)b * p.Nt + t) * Vs + s);
+  F[0] = fx;
+  F[1] = fy;
+}
+
+// The same force with one block per (slice, chain): the slice's angles are
+// staged in shared memory with 16-byte loads, sin(curl) is formed once per
+// plaquette (instead of three times per site), and each bond's force is the
+// difference of its two plaquettes' sines plus the tau term.  The arithmetic
+// of every term is that of boson_force_site, so the results are identical.
+// (x, y) of the sites s = threadIdx.x + k blockDim.x of an L x L slice,
+// advanced without integer division
+struct SiteWalk {
+  int s, x, y, dx, dy;
+  __device__ explicit SiteWalk(int L)
+      : s(threadIdx.x), x(threadIdx.x % L), y(threadIdx.x / L), dx(blockDim.x % L), dy(blockDim.x / L) {}
+  __device__ void next(int L) {
+    s += blockDim.x;
+    x += dx;
+    y += dy;
+    if (x >= L) {
+      x -= L;
+      ++y;
+    }
+  }
+};
+
+template <typename A>
+inline size_t boson_slice_smem(int L, int curls) {
+  return sizeof(A) * (size_t)L * L * (2 + curls);
+}
+
+template <typename A>
+__global__ void __launch_bounds__(256) k_boson_force_slice(BosonArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int L = p.L, Vs = L * L, Nt = p.Nt, t = blockIdx.x, b = blockIdx.y;
+  A* ph = reinterpret_cast<A*>(smem_raw);  // [Vs][2] angles of slice t
+  A* sc = ph + 2 * Vs;                     // [Vs] sin(curl)
+  const size_t sv = 2 * (size_t)Vs;
+  const A* phi = reinterpret_cast<const A*>(p.x) + (size_t)b * Nt * sv;
+  const float4* src = reinterpret_cast<const float4*>(phi + t * sv);
+  const int nvec = (int)(sv * sizeof(A) / 16);  // L even: whole 16-byte vectors
+  for (int i = threadIdx.x; i < nvec; i += blockDim.x) reinterpret_cast<float4*>(ph)[i] = __ldg(src + i);
+  __syncthreads();
+  for (SiteWalk w(L); w.s < Vs; w.next(L)) {
+    const int s = w.s, x = w.x, y = w.y;
+    const int xp = x + 1 == L ? 0 : x + 1, yp = y + 1 == L ? 0 : y + 1;
+    sc[s] = sin(ph[2 * (x + L * y)] + ph[2 * (xp + L * y) + 1] - ph[2 * (x + L * yp)] - ph[2 * (x + L * y) + 1]);
+  }
+  __syncthreads();
+  const Cx<A>* pn = reinterpret_cast<const Cx<A>*>(phi + ((t + 1) % Nt) * sv);
+  const Cx<A>* pp = reinterpret_cast<const Cx<A>*>(phi + ((t + Nt - 1) % Nt) * sv);
+  Cx<A>* F = reinterpret_cast<Cx<A>*>(p.F) + ((size_t)b * Nt + t) * Vs;
+  const A K = (A)p.K, ctau = (A)p.ctau;
+  for (SiteWalk w(L); w.s < Vs; w.next(L)) {
+    const int s = w.s, x = w.x, y = w.y;
+    const int xm = x == 0 ? L - 1 : x - 1, ym = y == 0 ? L - 1 : y - 1;
+    const A c = sc[s];
+    A fx = K * (c - sc[x + L * ym]);
+    A fy = K * (-c + sc[xm + L * y]);
+    const Cx<A> vn = pn[s], vp = pp[s];
+    const A v0 = ph[2 * s], v1 = ph[2 * s + 1];
+    if (p.compact) {
+      fx += ctau * -(-sin(vn.re - v0) + sin(v0 - vp.re));
+      fy += ctau * -(-sin(vn.im - v1) + sin(v1 - vp.im));
+    } else {
+      fx += ctau * -(-(vn.re - v0) + (v0 - vp.re));
+      fy += ctau * -(-(vn.im - v1) + (v1 - vp.im));
+    }
+    F[s] = mk<A>(fx, fy);
   }
 }
 
@@ -476,8 +664,21 @@ __global__ void k_cdot(const R* u, const R* v, int64_t n, double* out) {
   const R* ub = u + (size_t)b * 2 * n;
   const R* vb = v + (size_t)b * 2 * n;
   double acc = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    acc += (double)ub[2 * i] * (double)vb[2 * i] + (double)ub[2 * i + 1] * (double)vb[2 * i + 1];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t i0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if ((n & 1) == 0 && ((reinterpret_cast<uintptr_t>(ub) | reinterpret_cast<uintptr_t>(vb)) & 15) == 0) {
+    // two complex numbers per access
+    for (int64_t k = i0; 2 * k < n; k += stride) {
+      Cx<R> a0, a1, b0, b1;
+      ld2(ub + 4 * k, a0, a1);
+      ld2(vb + 4 * k, b0, b1);
+      acc += (double)a0.re * (double)b0.re + (double)a0.im * (double)b0.im + (double)a1.re * (double)b1.re +
+             (double)a1.im * (double)b1.im;
+    }
+  } else {
+    for (int64_t i = i0; i < n; i += stride)
+      acc += (double)ub[2 * i] * (double)vb[2 * i] + (double)ub[2 * i + 1] * (double)vb[2 * i + 1];
+  }
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) atomicAdd(out + b, acc);
 }
@@ -488,11 +689,11 @@ __global__ void k_boson_action(BosonArgs p, double* out) {
   __shared__ double sh[32];
   const int Vs = p.L * p.L;
   const int b = blockIdx.y;
-  const size_t n = (size_t)p.Nt * Vs;
+  const int n = p.Nt * Vs;  // sites of one chain (below 2^31)
   const A* phi = reinterpret_cast<const A*>(p.x) + (size_t)b * n * 2;
   const A* mom = p.F ? reinterpret_cast<const A*>(p.F) + (size_t)b * n * 2 : nullptr;
   double acc = 0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int s = i % Vs;
     const int t = i / Vs;
     const A* ph = phi + t * 2 * (size_t)Vs;
@@ -506,6 +707,42 @@ __global__ void k_boson_action(BosonArgs p, double* out) {
         const double q = mom[2 * i + c];
         acc += q * q / (2.0 * p.mass);
       }
+    }
+  }
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) atomicAdd(out + b, acc);
+}
+
+// The same sums with one block per (slice, chain), the slice staged in shared
+// memory with 16-byte loads.
+template <typename A>
+__global__ void __launch_bounds__(256) k_boson_action_slice(BosonArgs p, double* out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double sh[32];
+  const int L = p.L, Vs = L * L, Nt = p.Nt, t = blockIdx.x, b = blockIdx.y;
+  A* ph = reinterpret_cast<A*>(smem_raw);  // [Vs][2] angles of slice t
+  const size_t sv = 2 * (size_t)Vs;
+  const A* phi = reinterpret_cast<const A*>(p.x) + (size_t)b * Nt * sv;
+  const float4* src = reinterpret_cast<const float4*>(phi + t * sv);
+  const int nvec = (int)(sv * sizeof(A) / 16);
+  for (int i = threadIdx.x; i < nvec; i += blockDim.x) reinterpret_cast<float4*>(ph)[i] = __ldg(src + i);
+  __syncthreads();
+  const Cx<A>* pn = reinterpret_cast<const Cx<A>*>(phi + ((t + 1) % Nt) * sv);
+  const Cx<A>* mom = p.F ? reinterpret_cast<const Cx<A>*>(p.F) + ((size_t)b * Nt + t) * Vs : nullptr;
+  double acc = 0;
+  for (SiteWalk w(L); w.s < Vs; w.next(L)) {
+    const int s = w.s, x = w.x, y = w.y;
+    const int xp = x + 1 == L ? 0 : x + 1, yp = y + 1 == L ? 0 : y + 1;
+    acc += p.K * (double)cos(ph[2 * (x + L * y)] + ph[2 * (xp + L * y) + 1] - ph[2 * (x + L * yp)] -
+                             ph[2 * (x + L * y) + 1]);
+    const Cx<A> vn = pn[s];
+    const double d0 = (double)vn.re - (double)ph[2 * s], d1 = (double)vn.im - (double)ph[2 * s + 1];
+    acc += p.compact ? p.ctau * (1.0 - cos(d0)) : p.ctau * 0.5 * d0 * d0;
+    acc += p.compact ? p.ctau * (1.0 - cos(d1)) : p.ctau * 0.5 * d1 * d1;
+    if (mom) {
+      const Cx<A> q = mom[s];
+      acc += (double)q.re * (double)q.re / (2.0 * p.mass);
+      acc += (double)q.im * (double)q.im / (2.0 * p.mass);
     }
   }
   acc = block_sum(acc, sh);
@@ -652,9 +889,27 @@ template int launch_bvec<double, double>(BvecArgs, int, cudaStream_t);
 template <typename R>
 int launch_precon(const PreconArgs& a, cudaStream_t st) {
   const int Vs = a.L * a.L;
-  const int threads = 128;
-  dim3 grid((Vs / 2 + threads - 1) / threads, (a.Nt + a.TC - 1) / a.TC, a.bs);
-  k_precon<R><<<grid, threads, 0, st>>>(a);
+  const size_t band_smem = precon_band_smem(a.Nt);
+  if (band_smem <= smem_limit()) {
+    // a tau column per block, staged in shared memory; 16, 32 or 64 rows a
+    // thread, so that a block has at most 256 threads
+    constexpr int W = PRE_ROW_THREADS * 16 / (int)sizeof(Cx<R>);
+    dim3 grid((Vs + W - 1) / W, a.bs);
+    if (a.Nt <= 512) {
+      if (prepare_smem(k_precon_band<R, PRE_H, 16>, band_smem)) return QEDF_ERR_CUDA;
+      k_precon_band<R, PRE_H, 16><<<grid, PRE_ROW_THREADS * ((a.Nt + 15) / 16), band_smem, st>>>(a);
+    } else if (a.Nt <= 1024) {
+      if (prepare_smem(k_precon_band<R, PRE_H, 32>, band_smem)) return QEDF_ERR_CUDA;
+      k_precon_band<R, PRE_H, 32><<<grid, PRE_ROW_THREADS * ((a.Nt + 31) / 32), band_smem, st>>>(a);
+    } else {
+      if (prepare_smem(k_precon_band<R, PRE_H, 64>, band_smem)) return QEDF_ERR_CUDA;
+      k_precon_band<R, PRE_H, 64><<<grid, PRE_ROW_THREADS * ((a.Nt + 63) / 64), band_smem, st>>>(a);
+    }
+  } else {
+    const int threads = 128;
+    dim3 grid((Vs / 2 + threads - 1) / threads, (a.Nt + a.TC - 1) / a.TC, a.bs);
+    k_precon<R><<<grid, threads, 0, st>>>(a);
+  }
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
 template int launch_precon<float>(const PreconArgs&, cudaStream_t);
@@ -701,10 +956,15 @@ template int launch_force<double, double>(ForceArgs, int, cudaStream_t);
 
 template <typename A>
 int launch_boson_force(const BosonArgs& a, cudaStream_t st) {
-  const size_t n = (size_t)a.bs * a.Nt * a.L * a.L;
   const int threads = 256;
-  const int blocks = (int)std::min<size_t>((n + threads - 1) / threads, (size_t)num_sms() * 8);
-  k_boson_force<A><<<blocks, threads, 0, st>>>(a);
+  const size_t smem = boson_slice_smem<A>(a.L, 1);
+  if (smem <= smem_limit()) {
+    if (prepare_smem(k_boson_force_slice<A>, smem)) return QEDF_ERR_CUDA;
+    k_boson_force_slice<A><<<dim3(a.Nt, a.bs), threads, smem, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
+  }
+  dim3 grid((a.L * a.L + threads - 1) / threads, a.Nt, a.bs);
+  k_boson_force<A><<<grid, threads, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
 template int launch_boson_force<float>(const BosonArgs&, cudaStream_t);
@@ -725,8 +985,14 @@ template <typename A>
 int launch_boson_action(const BosonArgs& a, double* out, cudaStream_t st) {
   const size_t n = (size_t)a.Nt * a.L * a.L;
   const int threads = 256;
+  const size_t smem = boson_slice_smem<A>(a.L, 0);
+  if (smem + 32 * sizeof(double) <= smem_limit()) {
+    if (prepare_smem(k_boson_action_slice<A>, smem)) return QEDF_ERR_CUDA;
+    k_boson_action_slice<A><<<dim3(a.Nt, a.bs), threads, smem, st>>>(a, out);
+    return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
+  }
   const int bx = (int)std::max<size_t>(1, std::min<size_t>((n + threads - 1) / threads,
-                                                           (size_t)num_sms() * 4 / std::max(1, a.bs) + 1));
+                                                           (size_t)num_sms() * 16 / std::max(1, a.bs) + 1));
   k_boson_action<A><<<dim3(bx, a.bs), threads, 0, st>>>(a, out);
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
@@ -736,8 +1002,8 @@ template int launch_boson_action<double>(const BosonArgs&, double*, cudaStream_t
 template <typename R>
 int launch_cdot(const R* u, const R* v, int64_t n, int rows, double* out, cudaStream_t st) {
   const int threads = 256;
-  const int bx = (int)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads,
-                                                             (int64_t)num_sms() * 4 / std::max(1, rows) + 1));
+  const int bx = (int)std::max<int64_t>(1, std::min<int64_t>((n / 2 + threads - 1) / threads,
+                                                             (int64_t)num_sms() * 8 / std::max(1, rows) + 1));
   k_cdot<R><<<dim3(bx, rows), threads, 0, st>>>(u, v, n, out);
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }

@@ -150,6 +150,66 @@ def test_precon_vec_dropin(prec):
     assert relerr(got.cpu().numpy(), want) < (1e-6 if prec == "c64" else 1e-14)
 
 
+def _random_tau_csr(rng, Nt, per_row):
+    """a tau CSR with per_row unsorted random columns per row (no band form)"""
+    P = np.zeros((Nt, Nt))
+    for t in range(Nt):
+        cols = rng.choice(Nt, size=min(per_row, Nt), replace=False)
+        P[t, cols] = rng.standard_normal(len(cols))
+    return P
+
+
+@pytest.mark.parametrize("L,Nt,kind", [(6, 30, "band"), (4, 480, "band"), (48, 40, "band"), (6, 1100, "band"),
+                                       (4, 1900, "band"), (6, 64, "random"), (10, 1100, "random"),
+                                       (6, 480, "band_perturbed")])
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+def test_precon_apply_forms(prec, L, Nt, kind):
+    """The preconditioner kernel's banded form (bulk rows from a sliding
+    window), its per-row CSR form (boundary rows, other matrices) and the
+    fallback for long tau columns, against the oracle's dense product."""
+    from qed_fermion_b200 import ops
+    rng = np.random.default_rng(Nt + L)
+    if kind == "random":
+        P = _random_tau_csr(rng, Nt, 9)
+    else:
+        P = O.precon_tau_matrix(Nt).real.astype(np.float64)
+        if kind == "band_perturbed":  # one bulk row differs from the middle row
+            P[100, 101] += 0.25
+    rows, cols = np.nonzero(P)
+    row_ptr = np.concatenate([[0], np.cumsum(np.bincount(rows, minlength=Nt))]).astype(np.int32)
+    if kind == "random":  # unsorted columns within each row
+        order = np.lexsort((rng.random(len(rows)), rows))
+        rows, cols = rows[order], cols[order]
+    tau = (torch.tensor(row_ptr, device=DEV), torch.tensor(cols.astype(np.int32), device=DEV),
+           torch.tensor(P[rows, cols], device=DEV))
+    bs = 2
+    r = rng.standard_normal((bs, Nt * L * L)) + 1j * rng.standard_normal((bs, Nt * L * L))
+    want = O.precon_vec(r.reshape(bs, Nt, L * L), P).reshape(bs, -1)
+    cdt = torch.complex64 if prec == "c64" else torch.complex128
+    got = ops.precon_apply(torch.tensor(r, dtype=cdt, device=DEV), tau, L)
+    assert relerr(got.cpu().numpy(), want) < (1e-6 if prec == "c64" else 1e-14)
+
+
+@pytest.mark.parametrize("L,Nt", [(48, 8), (100, 4)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_boson_force_action_sizes(precision, L, Nt):
+    """Boson forces and actions at sizes that take the slice-staged kernels
+    (and, at L=100 in double precision, the per-site fallback) against the
+    oracle."""
+    from qed_fermion_b200.hmc import HmcSampler
+    rng = np.random.default_rng(L)
+    b = rng.uniform(-np.pi, np.pi, size=(2, 2, L, L, Nt))
+    hmc = HmcSampler(Lx=L, Ltau=Nt, bs=2, precision=precision, device=DEV)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    bt = torch.tensor(b, device=DEV)
+    cp = O.Couplings()
+    assert relerr(hmc.force_b_plaq_matfree(bt).cpu().numpy(), O.force_b_plaq(b, cp)) < tol
+    assert relerr(hmc.force_b_tau_noncmp(bt).cpu().numpy(), O.force_b_tau(b, cp)) < tol
+    assert relerr(hmc.force_b_tau_cmp(bt).cpu().numpy(), O.force_b_tau(b, O.Couplings(compact=True))) < tol
+    assert relerr(hmc.action_boson_plaq_matfree(bt).cpu().numpy(), O.action_boson_plaq(b, cp)) < tol
+    assert relerr(hmc.action_boson_tau(bt).cpu().numpy(), O.action_boson_tau(b, cp)) < tol
+
+
 @pytest.mark.parametrize("L,Nt,bs", [(4, 10, 1), (6, 20, 2), (12, 12, 1), (48, 4, 1), (66, 3, 1)])
 @pytest.mark.parametrize("prec", ["c64", "c128"])
 def test_force_matches_oracle(prec, L, Nt, bs):
