@@ -170,6 +170,7 @@ struct RhsState {
   double rr[PCG_MAX_RHS], res[PCG_MAX_RHS], resmax[PCG_MAX_RHS];
   int iters[PCG_MAX_RHS], lastru[PCG_MAX_RHS], status[PCG_MAX_RHS];
   unsigned char active[PCG_MAX_RHS], ru[PCG_MAX_RHS];
+  unsigned char pending[PCG_MAX_RHS];  // x += alpha p of the last iteration not yet applied
   int any_active, any_ru;
   double red[96];
 };
@@ -233,6 +234,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     st.status[v] = QEDF_OK;
     st.resmax[v] = 1.0;
     st.ru[v] = 0;
+    st.pending[v] = 0;
   }
   __syncthreads();
 
@@ -267,15 +269,14 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const int64_t base = vec_base(s, v);
     Cx<RS>* rsm = reinterpret_cast<Cx<RS>*>(dsm);
     const RS al = (RS)st.alpha[v];
-    const RS* pn = reinterpret_cast<const RS*>((st.iters[v] & 1) ? p.p1 : p.p0);
     const RS* opv = reinterpret_cast<const RS*>(Op);
     const int j = tid % PPR;
     const int rstep = blockDim.x / PPR;
     const bool jon = 2 * j < w;
     double acc_a = 0, acc_b = 0, acc_c = 0;
     if (sizeof(RS) == 4 && kind == 1) {
-      // The iteration update, single precision: the four input rows (p, Op,
-      // x, r) of this thread's next two rows are in flight while one row is
+      // The iteration update, single precision: the two input rows (Op, r)
+      // of this thread's next two rows are in flight while one row is
       // updated, as 16-byte cp.async copies into a two-stage area behind the
       // unit's r column (stage k & 1, [vector][thread] units).  A stage is
       // refilled only after its values were used.
@@ -285,30 +286,23 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       RS cpart = 0;  // this thread's |r|^2 in the iteration precision
       auto issue = [&](int k) {
         const int64_t i2 = 2 * (base + (int64_t)(t0 + k * rstep) * Vs + c0 + 2 * j);
-        uint4* d = stg + (size_t)(k & 1) * 4 * nthr + tid;
-        cp_async16(d, pn + i2);
-        cp_async16(d + nthr, opv + i2);
-        cp_async16(d + 2 * nthr, xs + i2);
-        cp_async16(d + 3 * nthr, r + i2);
+        uint4* d = stg + (size_t)(k & 1) * 2 * nthr + tid;
+        cp_async16(d, opv + i2);
+        cp_async16(d + nthr, r + i2);
         cp_async_commit();
       };
       if (K > 0) issue(0);
       if (K > 1) issue(1);
       for (int k = 0; k < K; ++k) {
         if (k + 1 < K) cp_async_wait<1>(); else cp_async_wait<0>();
-        const RS* d = reinterpret_cast<const RS*>(stg + (size_t)(k & 1) * 4 * nthr + tid);
-        Cx<RS> p0v, p1v, o0, o1, x0, x1, r0, r1;
-        ld2c(d, p0v, p1v);
-        ld2c(d + 4 * nthr, o0, o1);
-        ld2c(d + 8 * nthr, x0, x1);
-        ld2c(d + 12 * nthr, r0, r1);
-        x0 = mk<RS>(fma(al, p0v.re, x0.re), fma(al, p0v.im, x0.im));
-        x1 = mk<RS>(fma(al, p1v.re, x1.re), fma(al, p1v.im, x1.im));
+        const RS* d = reinterpret_cast<const RS*>(stg + (size_t)(k & 1) * 2 * nthr + tid);
+        Cx<RS> o0, o1, r0, r1;
+        ld2c(d, o0, o1);
+        ld2c(d + 4 * nthr, r0, r1);
         r0 = mk<RS>(fma(-al, o0.re, r0.re), fma(-al, o0.im, r0.im));
         r1 = mk<RS>(fma(-al, o1.re, r1.re), fma(-al, o1.im, r1.im));
         const int t = t0 + k * rstep;
         const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
-        st2(xs + i2, x0, x1);
         st2(r + i2, r0, r1);
         cpart = fma(r0.re, r0.re, fma(r0.im, r0.im, fma(r1.re, r1.re, fma(r1.im, r1.im, cpart))));
         st2(reinterpret_cast<RS*>(rsm + t * CHC + 2 * j), r0, r1);
@@ -331,16 +325,11 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         if (MIXED) st2(xh + i2, mk<RH>(0, 0), mk<RH>(0, 0));
         st2(r + i2, r0, r1);
       } else if (kind == 1) {
-        Cx<RS> p0v, p1v, o0, o1, x0, x1;
-        ld2c(pn + i2, p0v, p1v);
+        Cx<RS> o0, o1;
         ld2c(opv + i2, o0, o1);
-        ld2c(xs + i2, x0, x1);
         ld2c(r + i2, r0, r1);
-        x0 = mk<RS>(fma(al, p0v.re, x0.re), fma(al, p0v.im, x0.im));
-        x1 = mk<RS>(fma(al, p1v.re, x1.re), fma(al, p1v.im, x1.im));
         r0 = mk<RS>(fma(-al, o0.re, r0.re), fma(-al, o0.im, r0.im));
         r1 = mk<RS>(fma(-al, o1.re, r1.re), fma(-al, o1.im, r1.im));
-        st2(xs + i2, x0, x1);
         st2(r + i2, r0, r1);
       } else {
         ld2c(r + i2, r0, r1);
@@ -426,6 +415,11 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const A* phi = phi_all + S.phi0 + (S.shared ? 0 : (int64_t)(v - S.rhs0) * Nt * sv);
     const RS beta = (RS)st.beta[v];
     const bool has_old = st.iters[v] > 0;
+    // the previous iteration's x += alpha p, applied here on the slab's own
+    // slices while p_old is in registers anyway
+    const bool pend = st.pending[v];
+    const RS al_old = (RS)st.alpha[v];
+    RS* xl = xs + vb;
     const RS* pold = reinterpret_cast<const RS*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
     RS* pnew = reinterpret_cast<RS*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
     const RS* zz = (S.precon ? zbuf : reinterpret_cast<const RS*>(r)) + vb;
@@ -434,12 +428,24 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     Cx<RS> X0[BY][2], X1[BY][2], Y[BY][2];
     Cx<RS> Yp[STASH_S ? 1 : BY][2];
     double pap = 0;
-    auto getp = [&](Cx<RS> (&X)[BY][2], int t) {
+    auto getp = [&](Cx<RS> (&X)[BY][2], int t, bool own) {
       if (!E.on) return;
       E.load_coherent(X, zz + t * sv);
       if (has_old) {
         Cx<RS> T0[BY][2];
         E.load_coherent(T0, pold + t * sv);
+        if (own && pend) {
+          Cx<RS> XL[BY][2];
+          E.load_coherent(XL, xl + t * sv);
+#pragma unroll
+          for (int q = 0; q < BY; ++q)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              XL[q][c].re = fma(al_old, T0[q][c].re, XL[q][c].re);
+              XL[q][c].im = fma(al_old, T0[q][c].im, XL[q][c].im);
+            }
+          E.store(xl + t * sv, XL);
+        }
 #pragma unroll
         for (int q = 0; q < BY; ++q)
 #pragma unroll
@@ -450,8 +456,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       }
     };
     const int tp = (a - 1 + Nt) % Nt;
-    getp(X0, tp);
-    getp(X1, a);
+    getp(X0, tp, false);
+    getp(X1, a, true);
     if (E.on) E.store(pnew + a * sv, X1);
     A ang[BY][4];
     if constexpr (!PHS_S) E.load_angles(ang, phi + a * sv);
@@ -462,7 +468,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     copy_blk<RS, BY>(X0, X1);
     for (int t = a; t < bnd; ++t) {
       const int tn = (t + 1) % Nt;
-      getp(X1, tn);
+      getp(X1, tn, t + 1 < bnd);
       if (E.on && t + 1 < bnd) E.store(pnew + tn * sv, X1);
       if constexpr (!PHS_S) {
         E.phases_from(ang, t1, th);
@@ -567,11 +573,24 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     __syncthreads();
   };
 
-  // x (double) += x_lo; x_lo = 0   for the flagged right-hand sides
+  // the pending x += alpha p_last of right-hand side v at one site pair
+  auto apply_pending = [&](int v, int64_t i2, Cx<RS>& l0, Cx<RS>& l1) {
+    if (!st.pending[v]) return;
+    const RS* pl = reinterpret_cast<const RS*>((st.iters[v] & 1) ? p.p0 : p.p1);  // p of the last iteration
+    const RS al = (RS)st.alpha[v];
+    Cx<RS> p0v, p1v;
+    ld2c(pl + i2, p0v, p1v);
+    l0 = mk<RS>(fma(al, p0v.re, l0.re), fma(al, p0v.im, l0.im));
+    l1 = mk<RS>(fma(al, p1v.re, l1.re), fma(al, p1v.im, l1.im));
+  };
+
+  // x (double) += x_lo (+ the pending update); x_lo = 0   for the flagged
+  // right-hand sides (all_active: every one still active or with a pending
+  // update, at the end of the solve)
   auto fold_unit = [&](int u, bool all_active) {
     int s, v, c0, c1;
     unitE(u, s, v, c0, c1);
-    if (!(all_active ? st.active[v] : st.ru[v])) return;
+    if (!(all_active ? (st.active[v] || st.pending[v]) : st.ru[v])) return;
     const PcgSys& S = p.sys[s];
     const int Vs = SL(S) * SL(S), w = c1 - c0;
     const int64_t base = vec_base(s, v);
@@ -582,6 +601,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       Cx<RS> l0, l1;
       Cx<RH> h0, h1;
       ld2c(xs + i2, l0, l1);
+      apply_pending(v, i2, l0, l1);
       ld2c(xh + i2, h0, h1);
       h0.re += (RH)l0.re;
       h0.im += (RH)l0.im;
@@ -589,6 +609,25 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       h1.im += (RH)l1.im;
       st2(xh + i2, h0, h1);
       st2(xs + i2, mk<RS>(0, 0), mk<RS>(0, 0));
+    }
+  };
+
+  // plain modes, end of the solve: x += alpha p_last where still pending
+  auto flush_unit = [&](int u) {
+    int s, v, c0, c1;
+    unitE(u, s, v, c0, c1);
+    if (!st.pending[v]) return;
+    const PcgSys& S = p.sys[s];
+    const int Vs = SL(S) * SL(S), w = c1 - c0;
+    const int64_t base = vec_base(s, v);
+    const int j = tid % PPR;
+    if (2 * j >= w) return;
+    for (int t = tid / PPR; t < S.Nt; t += blockDim.x / PPR) {
+      const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
+      Cx<RS> l0, l1;
+      ld2c(xs + i2, l0, l1);
+      apply_pending(v, i2, l0, l1);
+      st2(xs + i2, l0, l1);
     }
   };
 
@@ -669,6 +708,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
       for (int v = tid; v < NV; v += blockDim.x) {
         if (!st.ru[v]) continue;
+        st.pending[v] = 0;  // folded into x above
         st.rr[v] = acc.ru_rr[v];
         st.rz[v] = acc.ru_rz[v];
         const double res = sqrt(st.rr[v] / acc.bb[v]);
@@ -710,7 +750,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     pc.lap(2);
 
     // ---- phase BC
-    for (int v = tid; v < NV; v += blockDim.x) st.alpha[v] = st.rz[v] / acc.pAp[aslot * NV + v];
+    // alpha of inactive systems stays that of their last iteration: a pending
+    // x update still uses it
+    for (int v = tid; v < NV; v += blockDim.x)
+      if (st.active[v]) st.alpha[v] = st.rz[v] / acc.pAp[aslot * NV + v];
     __syncthreads();
     for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) {
       int s, v, c0, c1;
@@ -729,6 +772,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       st.rz[v] = acc.rz[slot * NV + v];
       st.rr[v] = acc.rr[slot * NV + v];
       st.iters[v] += 1;
+      st.pending[v] = 1;
     }
     __syncthreads();
     ++it;
@@ -738,9 +782,12 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     pc.prof[7] += clock64() - t_begin;
   }
 
-  // mixed: fold the remaining float updates of unconverged systems into x
+  // mixed: fold the remaining float updates of unconverged systems into x;
+  // plain: apply the last iteration's x update
   if (MIXED && ok) {
     for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) fold_unit(u, true);
+  } else if (ok) {
+    for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) flush_unit(u);
   }
   if (blockIdx.x == 0) {
     const unsigned int err = *((volatile unsigned int*)(p.bar + 2));
@@ -900,7 +947,7 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   // elementwise units: the r column, and in single precision the two-stage
   // area of the update pass
   smem = std::max(smem, ((sizeof(Cx<RS>) * (size_t)Ntmax * PCG_CHUNK + 15) / 16 * 16) +
-                            (sizeof(RS) == 4 ? 2 * 4 * 16 * (size_t)threads : 0));
+                            (sizeof(RS) == 4 ? 2 * 2 * 16 * (size_t)threads : 0));
   if (smem + sizeof(RhsState) > 227 * 1024) return QEDF_ERR_SIZE;
   auto kern = k_pcg<RS, RH, A, BY, ECS, ECH>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
