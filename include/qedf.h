@@ -144,6 +144,30 @@ int qedf_cdot_c128(const double* u, const double* v, int64_t n, int rows, double
                    qedf_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Bond-bond correlators of the stochastic estimator (T1 :1393, T21 :1447,
+ * T2 :1504, T4 :1561 of stochastic_estimator.py): the passes before and after
+ * the 2-D FFTs of the pair sums.
+ *
+ * qedf_bb_pair_fields: for pairs p < npairs, (s, t) = (ps[p], pt[p]), writes
+ * fa[p][tau][y][x] and fb[p][tau][y][x], the two fields whose transforms the
+ * reference multiplies (kind 1: T1, 21: T21, 2: T2, 4: T4), from eta and G_eta
+ * [Nrv][Ltau][Lx*Lx] (complex; conj(eta) is taken here) and ephase = e^{i phi_x}
+ * [Ltau][Lx*Lx].  npairs <= 65535 per call.
+ * qedf_bb_kspace_acc: S[k] += sum_i A[i][k] B[i][k] for rows i < rows of Vs
+ * complex entries; S is complex128 [Vs], accumulated in double precision.
+ * ------------------------------------------------------------------------- */
+int qedf_bb_pair_fields_c64(int kind, const float* eta, const float* g_eta, const float* ephase, const int* ps,
+                            const int* pt, int npairs, int Nrv, int Lx, int Ltau, float* fa, float* fb,
+                            qedf_stream_t stream);
+int qedf_bb_pair_fields_c128(int kind, const double* eta, const double* g_eta, const double* ephase,
+                             const int* ps, const int* pt, int npairs, int Nrv, int Lx, int Ltau, double* fa,
+                             double* fb, qedf_stream_t stream);
+int qedf_bb_kspace_acc_c64(const float* A, const float* B, int64_t rows, int Vs, double* S,
+                           qedf_stream_t stream);
+int qedf_bb_kspace_acc_c128(const double* A, const double* B, int64_t rows, int Vs, double* S,
+                            qedf_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Batched preconditioned CG on M^dag M x = b (persistent kernel).
  *
  * Replaces preconditioned_cg_fast_test (hmc_sampler_batch.py:751-846) and the

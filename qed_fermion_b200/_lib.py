@@ -61,6 +61,9 @@ for _prec in ("c64", "c128"):
     SIGNATURES[f"qedf_b_vec_per_tau_{_prec}"] = (c_int, [_vp, _vp, _vp, c_int, c_int, c_double, c_int, _vp])
     SIGNATURES[f"qedf_precon_vec_{_prec}"] = (c_int, [_vp, _vp, c_int, c_int, c_int, _vp, _vp, _vp, _vp])
     SIGNATURES[f"qedf_cdot_{_prec}"] = (c_int, [_vp, _vp, c_int64, c_int, _vp, _vp])
+    SIGNATURES[f"qedf_bb_pair_fields_{_prec}"] = (
+        c_int, [c_int, _vp, _vp, _vp, _vp, _vp, c_int, c_int, c_int, c_int, _vp, _vp, _vp])
+    SIGNATURES[f"qedf_bb_kspace_acc_{_prec}"] = (c_int, [_vp, _vp, c_int64, c_int, _vp, _vp])
 for _r in ("f32", "f64"):
     SIGNATURES[f"qedf_boson_force_{_r}"] = (c_int, [_vp, _vp, c_int, c_int, c_int, c_double, c_double, c_int, _vp])
     SIGNATURES[f"qedf_boson_action_{_r}"] = (

@@ -1,0 +1,197 @@
+// Bond-bond correlators of the stochastic estimator: the two passes around
+// the 2-D FFTs of the pair-averaged correlation functions T1, T21, T2 and T4
+// (stochastic_estimator.py: T1 :1393, T21 :1447, T2 :1504, T4 :1561).
+//
+// For every noise pair s < t and slice tau the reference forms two fields on
+// the spatial slice, a_st(r) and b_st(r) (products of conj(eta), G_eta and
+// e^{+-i phi_x}, some at r + x), and sums
+//     ifft2(a_st) * fft2(b_st)
+// over pairs and slices before one inverse transform gives the correlation
+// in real space.  Here
+//   qedf_bb_pair_fields  writes a_st and b_st of a chunk of pairs in one pass
+//                        (the torch formulation needs a gather, a roll and a
+//                        product per factor, each a pass over the chunk);
+//   qedf_bb_kspace_acc   accumulates sum_rows A(k) B(k) in double precision
+//                        from the two transforms (cuFFT, called by the host).
+// Both are HBM-bound: 2 complex writes per pair-site and 2 complex reads per
+// pair-site respectively; the inputs eta, G_eta of one slice are reread from
+// L2 by every pair.
+#include <algorithm>
+
+#include "qedf_common.cuh"
+#include "qedf_internal.h"
+
+namespace qedf {
+
+namespace {
+
+struct BondArgs {
+  int kind;  // 1: T1, 21: T21, 2: T2, 4: T4
+  const void* eta;
+  const void* g;
+  const void* ep;  // e^{i phi_x} per site, [Ltau][Vs]
+  const int* ps;
+  const int* pt;
+  int npairs, nrv, L, Nt;
+  void* fa;
+  void* fb;
+};
+
+template <typename R>
+__device__ __forceinline__ Cx<R> ldcx(const R* base, int64_t i) {
+  return *reinterpret_cast<const Cx<R>*>(base + 2 * i);
+}
+template <typename R>
+__device__ __forceinline__ Cx<R> conjc(Cx<R> a) {
+  return mk<R>(a.re, -a.im);
+}
+
+// one thread per (pair, site of the chunk's slices); grid (sites / 256, pairs)
+template <typename R>
+__global__ void __launch_bounds__(256) k_bb_pair_fields(BondArgs a) {
+  const int Vs = a.L * a.L;
+  const int64_t nsite = (int64_t)a.Nt * Vs;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsite) return;
+  const int p = blockIdx.y;
+  const int s = a.ps[p], t = a.pt[p];
+  const int64_t o = (int64_t)p * nsite + i;
+  if ((unsigned)s >= (unsigned)a.nrv || (unsigned)t >= (unsigned)a.nrv) {  // not a noise vector: zero fields
+    *reinterpret_cast<Cx<R>*>(reinterpret_cast<R*>(a.fa) + 2 * o) = mk<R>(0, 0);
+    *reinterpret_cast<Cx<R>*>(reinterpret_cast<R*>(a.fb) + 2 * o) = mk<R>(0, 0);
+    return;
+  }
+  const int tau = (int)(i / Vs), site = (int)(i - (int64_t)tau * Vs);
+  const int y = site / a.L, x = site - y * a.L;
+  const int64_t r = i, r1 = (int64_t)tau * Vs + y * a.L + (x + 1 == a.L ? 0 : x + 1);
+  const R* eta = reinterpret_cast<const R*>(a.eta);
+  const R* g = reinterpret_cast<const R*>(a.g);
+  const int64_t os = (int64_t)s * nsite, ot = (int64_t)t * nsite;
+  const Cx<R> ep = ldcx(reinterpret_cast<const R*>(a.ep), r);
+  Cx<R> A, B;
+  if (a.kind == 1) {
+    // a = ec_s g_t(r+x) e,  b = g_s(r+x) ec_t e
+    A = cmul(cmul(conjc(ldcx(eta, os + r)), ldcx(g, ot + r1)), ep);
+    B = cmul(cmul(ldcx(g, os + r1), conjc(ldcx(eta, ot + r))), ep);
+  } else if (a.kind == 4) {
+    // a = ec_s(r+x) g_t e*,  b = g_s ec_t(r+x) e*
+    const Cx<R> em = conjc(ep);
+    A = cmul(cmul(conjc(ldcx(eta, os + r1)), ldcx(g, ot + r)), em);
+    B = cmul(cmul(ldcx(g, os + r), conjc(ldcx(eta, ot + r1))), em);
+  } else {
+    const Cx<R> ecs = conjc(ldcx(eta, os + r)), ecs1 = conjc(ldcx(eta, os + r1));
+    const Cx<R> ect = conjc(ldcx(eta, ot + r)), ect1 = conjc(ldcx(eta, ot + r1));
+    const Cx<R> gs = ldcx(g, os + r), gs1 = ldcx(g, os + r1);
+    const Cx<R> gt = ldcx(g, ot + r), gt1 = ldcx(g, ot + r1);
+    const R h = (R)0.5;
+    if (a.kind == 21) {
+      // a = (ec_s(r+x) g_t + ec_t(r+x) g_s) e* / 2,  b = (g_s(r+x) ec_t + g_t(r+x) ec_s) e / 2
+      A = h * cmul(cmul(ecs1, gt) + cmul(ect1, gs), conjc(ep));
+      B = h * cmul(cmul(gs1, ect) + cmul(gt1, ecs), ep);
+    } else {
+      // T2: a = (ec_s g_t(r+x) + ec_t g_s(r+x)) e / 2,  b = (g_s ec_t(r+x) + g_t ec_s(r+x)) e* / 2
+      A = h * cmul(cmul(ecs, gt1) + cmul(ect, gs1), ep);
+      B = h * cmul(cmul(gs, ect1) + cmul(gt, ecs1), conjc(ep));
+    }
+  }
+  *reinterpret_cast<Cx<R>*>(reinterpret_cast<R*>(a.fa) + 2 * o) = A;
+  *reinterpret_cast<Cx<R>*>(reinterpret_cast<R*>(a.fb) + 2 * o) = B;
+}
+
+// S[k] += sum_i A[i][k] B[i][k] over n rows of Vs columns, in double.
+// Block (32 columns) x (8 row lanes); the row lanes are summed in shared
+// memory and each block adds its column sums with two atomics per column.
+template <typename R>
+__global__ void __launch_bounds__(256) k_bb_kspace_acc(const R* A, const R* B, int64_t n, int Vs, double* S) {
+  __shared__ double red[2][8][33];
+  const int cx = threadIdx.x & 31, ry = threadIdx.x >> 5;
+  const int k = blockIdx.x * 32 + cx;
+  double sr = 0, si = 0;
+  if (k < Vs) {
+    for (int64_t i = (int64_t)blockIdx.y * 8 + ry; i < n; i += (int64_t)gridDim.y * 8) {
+      const Cx<R> u = ldcx(A, i * Vs + k), v = ldcx(B, i * Vs + k);
+      const double ur = u.re, ui = u.im, vr = v.re, vi = v.im;
+      sr = fma(ur, vr, fma(-ui, vi, sr));
+      si = fma(ur, vi, fma(ui, vr, si));
+    }
+  }
+  red[0][ry][cx] = sr;
+  red[1][ry][cx] = si;
+  __syncthreads();
+  if (ry == 0 && k < Vs) {
+    double tr = 0, ti = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      tr += red[0][q][cx];
+      ti += red[1][q][cx];
+    }
+    atomicAdd(S + 2 * k, tr);
+    atomicAdd(S + 2 * k + 1, ti);
+  }
+}
+
+template <typename R>
+int pair_fields_entry(int kind, const R* eta, const R* g, const R* ep, const int* ps, const int* pt, int npairs,
+                      int Nrv, int Lx, int Ltau, R* fa, R* fb, cudaStream_t st) {
+  if (kind != 1 && kind != 21 && kind != 2 && kind != 4) return QEDF_ERR_ARG;
+  if (!eta || !g || !ep || !ps || !pt || !fa || !fb) return QEDF_ERR_ARG;
+  if (npairs < 0 || npairs > 65535 || Lx < 1 || Ltau < 1 || Nrv < 2) return QEDF_ERR_ARG;
+  if (npairs == 0) return QEDF_OK;
+  const int64_t nsite = (int64_t)Ltau * Lx * Lx;
+  BondArgs a;
+  a.kind = kind;
+  a.eta = eta;
+  a.g = g;
+  a.ep = ep;
+  a.ps = ps;
+  a.pt = pt;
+  a.npairs = npairs;
+  a.nrv = Nrv;
+  a.L = Lx;
+  a.Nt = Ltau;
+  a.fa = fa;
+  a.fb = fb;
+  dim3 grid((unsigned)((nsite + 255) / 256), npairs);
+  k_bb_pair_fields<R><<<grid, 256, 0, st>>>(a);
+  return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
+}
+
+template <typename R>
+int kspace_acc_entry(const R* A, const R* B, int64_t rows, int Vs, double* S, cudaStream_t st) {
+  if (!A || !B || !S || rows < 0 || Vs < 1) return QEDF_ERR_ARG;
+  if (rows == 0) return QEDF_OK;
+  const int bx = (Vs + 31) / 32;
+  const int64_t want = std::max<int64_t>(1, (int64_t)num_sms() * 8 / bx);
+  const int by = (int)std::min<int64_t>(std::min<int64_t>(want, (rows + 7) / 8), 65535);
+  k_bb_kspace_acc<R><<<dim3(bx, by), 256, 0, st>>>(A, B, rows, Vs, S);
+  return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
+}
+
+}  // namespace
+}  // namespace qedf
+
+using namespace qedf;
+
+extern "C" {
+
+int qedf_bb_pair_fields_c64(int kind, const float* eta, const float* g_eta, const float* ephase, const int* ps,
+                            const int* pt, int npairs, int Nrv, int Lx, int Ltau, float* fa, float* fb,
+                            qedf_stream_t s) {
+  return pair_fields_entry<float>(kind, eta, g_eta, ephase, ps, pt, npairs, Nrv, Lx, Ltau, fa, fb,
+                                  reinterpret_cast<cudaStream_t>(s));
+}
+int qedf_bb_pair_fields_c128(int kind, const double* eta, const double* g_eta, const double* ephase,
+                             const int* ps, const int* pt, int npairs, int Nrv, int Lx, int Ltau, double* fa,
+                             double* fb, qedf_stream_t s) {
+  return pair_fields_entry<double>(kind, eta, g_eta, ephase, ps, pt, npairs, Nrv, Lx, Ltau, fa, fb,
+                                   reinterpret_cast<cudaStream_t>(s));
+}
+int qedf_bb_kspace_acc_c64(const float* A, const float* B, int64_t rows, int Vs, double* S, qedf_stream_t s) {
+  return kspace_acc_entry<float>(A, B, rows, Vs, S, reinterpret_cast<cudaStream_t>(s));
+}
+int qedf_bb_kspace_acc_c128(const double* A, const double* B, int64_t rows, int Vs, double* S,
+                            qedf_stream_t s) {
+  return kspace_acc_entry<double>(A, B, rows, Vs, S, reinterpret_cast<cudaStream_t>(s));
+}
+
+}  // extern "C"

@@ -12,7 +12,10 @@ order) and over tau, the spatial correlation of two bond products,
 evaluated with 2-D FFTs over (y, x).  Because the inverse transform is linear,
 the products of the transforms are summed over pairs and tau first and only
 one inverse FFT per observable remains; the reference instead transforms back
-per batch.  Pairs are processed in chunks sized by ``chunk_bytes``.
+per batch.  Pairs are processed in chunks sized by ``chunk_bytes``: per chunk
+one kernel writes both fields of every pair (``ops.bb_pair_fields``), cuFFT
+transforms them, and one kernel adds the products of the transforms into a
+double-precision k-space sum (``ops.bb_kspace_acc``).
 
 Layouts as in the reference: eta, G_eta ``[Nrv, Ltau * Ly * Lx]`` (index
 tau Vs + x + Lx y); boson ``[1, 2, Lx, Ly, Ltau]``.  Inputs must be CUDA
@@ -21,6 +24,8 @@ tensors; the transforms are cuFFT's (through torch).
 from __future__ import annotations
 
 import torch
+
+from . import ops
 
 
 class BondBond:
@@ -48,43 +53,50 @@ class BondBond:
         per = ec[0].numel() * ec.element_size() * n_arrays
         return max(1, self.chunk_bytes // max(1, per))
 
-    def _pair_mean(self, ec, fa, fb):
-        nrv = ec.shape[0]
-        pairs = torch.combinations(torch.arange(nrv, device=ec.device), r=2, with_replacement=False)
-        S = torch.zeros((self.Ly, self.Lx), dtype=ec.dtype, device=ec.device)
-        for ch in pairs.split(self._chunk(ec)):
-            s, t = ch[:, 0], ch[:, 1]
-            aF = torch.fft.ifft2(fa(s, t), norm="backward")
-            bF = torch.fft.fft2(fb(s, t), norm="forward")
-            S += (aF * bF).sum(dim=(0, 1))
-        return torch.fft.ifft2(S, norm="forward") / (len(pairs) * self.Ltau)
+    def _pair_mean(self, kind, eta, G_eta, boson):
+        """mean over pairs s < t and tau of ifft2(a_st) * fft2(b_st), transformed
+        back to real space; a_st, b_st are the fields of correlator ``kind``."""
+        dt = eta.dtype
+        nrv = eta.shape[0]
+        if nrv < 2:
+            raise RuntimeError("bond-bond correlators need at least two noise vectors")
+        e = eta.resolve_conj().reshape(nrv, -1).contiguous()
+        g = G_eta.to(dt).resolve_conj().reshape(nrv, -1).contiguous()
+        ph = boson.permute(0, 1, 4, 3, 2)[0, 0].to(e.real.dtype)
+        ep = torch.exp(1j * ph).to(dt).contiguous()
+        Vs = self.Lx * self.Ly
+        pairs = torch.combinations(torch.arange(nrv, device=e.device), r=2, with_replacement=False).to(torch.int32)
+        chunk = min(65535, self._chunk(e.reshape(nrv, self.Ltau, self.Ly, self.Lx)), len(pairs))
+        fa = torch.empty((chunk, self.Ltau, self.Ly, self.Lx), dtype=dt, device=e.device)
+        fb = torch.empty_like(fa)
+        S = torch.zeros(Vs, dtype=torch.complex128, device=e.device)
+        for ch in pairs.split(chunk):
+            n = len(ch)
+            a, b = fa[:n], fb[:n]
+            ops.bb_pair_fields(kind, e, g, ep, ch[:, 0].contiguous(), ch[:, 1].contiguous(), self.Lx, a, b)
+            # unnormalised transforms; the 1 / Vs of each is applied to S once
+            ops.bb_kspace_acc(torch.fft.ifft2(a, norm="forward"), torch.fft.fft2(b, norm="backward"), S)
+        S = S.view(self.Ly, self.Lx) / (Vs * Vs)
+        return (torch.fft.ifft2(S, norm="forward") / (len(pairs) * self.Ltau)).to(dt)
 
     # ---- the correlators ----------------------------------------------------
     def T1(self, eta, G_eta, boson):
         ec, g, ph = self._fields(eta, G_eta, boson)
         e = torch.exp(1j * ph)
         sx = self._sx
-        out = -self._pair_mean(ec, lambda s, t: ec[s] * sx(g[t], 1) * e, lambda s, t: sx(g[s], 1) * ec[t] * e)
+        out = -self._pair_mean("T1", eta, G_eta, boson)
         out[0, -1] += (sx(g, 1) * torch.roll(ec, 1, dims=-1) * e * torch.exp(1j * torch.roll(ph, 1, dims=-1))).mean()
         return out
 
     def T21(self, eta, G_eta, boson):
         ec, g, ph = self._fields(eta, G_eta, boson)
-        em, ep = torch.exp(-1j * ph), torch.exp(1j * ph)
-        sx = self._sx
-        out = -self._pair_mean(
-            ec, lambda s, t: (sx(ec[s], 1) * g[t] + sx(ec[t], 1) * g[s]) * em / 2,
-            lambda s, t: (sx(g[s], 1) * ec[t] + sx(g[t], 1) * ec[s]) * ep / 2)
+        out = -self._pair_mean("T21", eta, G_eta, boson)
         out[0, 0] += (g * ec).mean()
         return out
 
     def T2(self, eta, G_eta, boson):
         ec, g, ph = self._fields(eta, G_eta, boson)
-        em, ep = torch.exp(-1j * ph), torch.exp(1j * ph)
-        sx = self._sx
-        out = -self._pair_mean(
-            ec, lambda s, t: (ec[s] * sx(g[t], 1) + ec[t] * sx(g[s], 1)) * ep / 2,
-            lambda s, t: (g[s] * sx(ec[t], 1) + g[t] * sx(ec[s], 1)) * em / 2)
+        out = -self._pair_mean("T2", eta, G_eta, boson)
         out[0, 0] += (g * ec).mean()
         return out
 
@@ -92,7 +104,7 @@ class BondBond:
         ec, g, ph = self._fields(eta, G_eta, boson)
         e = torch.exp(-1j * ph)
         sx = self._sx
-        out = -self._pair_mean(ec, lambda s, t: sx(ec[s], 1) * g[t] * e, lambda s, t: g[s] * sx(ec[t], 1) * e)
+        out = -self._pair_mean("T4", eta, G_eta, boson)
         out[0, 1] += (g * sx(ec, 2) * e * torch.exp(-1j * sx(ph, 1))).mean()
         return out
 

@@ -151,6 +151,46 @@ def cdot(u: torch.Tensor, v: torch.Tensor, out: torch.Tensor = None) -> torch.Te
     return out
 
 
+BB_KINDS = {"T1": 1, "T21": 21, "T2": 2, "T4": 4}
+
+
+def bb_pair_fields(kind: str, eta: torch.Tensor, g_eta: torch.Tensor, ephase: torch.Tensor, ps: torch.Tensor,
+                   pt: torch.Tensor, Lx: int, fa: torch.Tensor, fb: torch.Tensor) -> None:
+    """Fill ``fa``, ``fb`` ``[npairs, Ltau, Ly, Lx]`` with the two fields of the
+    bond-bond correlator ``kind`` ("T1", "T21", "T2", "T4") for the noise pairs
+    (ps[p], pt[p]); eta, G_eta ``[Nrv, Ltau*Vs]`` (same complex dtype, conj(eta)
+    is taken by the kernel), ephase = e^{i phi_x} ``[Ltau, Ly, Lx]``."""
+    _check_cuda(eta, g_eta, ephase, ps, pt, fa, fb)
+    prec, _ = _PREC[eta.dtype]
+    for t in (g_eta, ephase, fa, fb):
+        if t.dtype != eta.dtype or not t.is_contiguous() or t.is_conj():
+            raise RuntimeError("bb_pair_fields: complex tensors must share eta's dtype and be contiguous")
+    if ps.dtype != torch.int32 or pt.dtype != torch.int32 or not ps.is_contiguous() or not pt.is_contiguous():
+        raise RuntimeError("bb_pair_fields: pair indices must be contiguous int32")
+    nrv, N = eta.shape
+    Vs, Ltau = lattice_dims(N, Lx)
+    npairs = ps.numel()
+    if fa.numel() < npairs * N or fb.numel() < npairs * N or ephase.numel() != N or pt.numel() != npairs:
+        raise RuntimeError("bb_pair_fields: buffer sizes do not match")
+    _lib.call(f"qedf_bb_pair_fields_{prec}", BB_KINDS[kind], ptr(eta), ptr(g_eta), ptr(ephase), ptr(ps), ptr(pt),
+              npairs, nrv, Lx, Ltau, ptr(fa), ptr(fb), stream_handle())
+
+
+def bb_kspace_acc(A: torch.Tensor, B: torch.Tensor, S: torch.Tensor) -> None:
+    """S[k] += sum over rows of A[..., k] B[..., k] (the last two dimensions of
+    A, B are the spatial modes), accumulated in double precision into the
+    complex128 ``S`` of Vs entries."""
+    _check_cuda(A, B, S)
+    prec, _ = _PREC[A.dtype]
+    if B.dtype != A.dtype or S.dtype != torch.complex128 or not (A.is_contiguous() and B.is_contiguous()
+                                                                  and S.is_contiguous()):
+        raise RuntimeError("bb_kspace_acc: contiguous A, B of one dtype and a complex128 S are required")
+    Vs = S.numel()
+    if A.numel() != B.numel() or A.numel() % Vs:
+        raise RuntimeError("bb_kspace_acc: sizes do not match")
+    _lib.call(f"qedf_bb_kspace_acc_{prec}", ptr(A), ptr(B), A.numel() // Vs, Vs, ptr(S), stream_handle())
+
+
 def _rprec(t):
     if t.dtype == torch.float32:
         return "f32"

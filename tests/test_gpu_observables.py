@@ -74,3 +74,49 @@ def test_cpu_tensors_are_refused():
     with pytest.raises(RuntimeError):
         bb.T1(torch.zeros(3, 96, dtype=torch.complex128), torch.zeros(3, 96, dtype=torch.complex128),
               torch.zeros(1, 2, 4, 4, 6))
+
+
+def _fields_torch(kind, eta, g, ep, s, t):
+    """the two pair fields of a correlator, written with torch for the check
+    (x-shift by one site: roll by -1 along x)"""
+    ec = eta.conj()
+    sx = lambda a: torch.roll(a, shifts=-1, dims=-1)
+    em = ep.conj()
+    if kind == "T1":
+        return ec[s] * sx(g[t]) * ep, sx(g[s]) * ec[t] * ep
+    if kind == "T4":
+        return sx(ec[s]) * g[t] * em, g[s] * sx(ec[t]) * em
+    if kind == "T21":
+        return ((sx(ec[s]) * g[t] + sx(ec[t]) * g[s]) * em / 2, (sx(g[s]) * ec[t] + sx(g[t]) * ec[s]) * ep / 2)
+    return ((ec[s] * sx(g[t]) + ec[t] * sx(g[s])) * ep / 2, (g[s] * sx(ec[t]) + g[t] * sx(ec[s])) * em / 2)
+
+
+@pytest.mark.parametrize("kind", ["T1", "T21", "T2", "T4"])
+@pytest.mark.parametrize("cdt,tol", [(torch.complex128, 1e-14), (torch.complex64, 1e-6)])
+def test_pair_fields_and_kspace_sum_kernels(kind, cdt, tol):
+    """The pair-field kernel against torch products for every correlator, with
+    an out-of-range pair index giving zero fields; the k-space sum against a
+    torch sum of the transforms' products."""
+    from qed_fermion_b200 import ops
+    L, Nt, nrv = 6, 5, 4
+    gen = torch.Generator(device="cpu").manual_seed(3)
+    mk = lambda *sh: torch.complex(torch.randn(*sh, generator=gen, dtype=torch.float64),
+                                    torch.randn(*sh, generator=gen, dtype=torch.float64)).to(cdt).to(DEV)
+    eta, g = mk(nrv, Nt, L, L), mk(nrv, Nt, L, L)
+    ep = torch.exp(1j * torch.rand(Nt, L, L, generator=gen, dtype=torch.float64) * 6.2832).to(cdt).to(DEV)
+    pairs = torch.combinations(torch.arange(nrv), r=2).to(torch.int32)
+    pairs = torch.cat([pairs, torch.tensor([[0, nrv]], dtype=torch.int32)]).to(DEV)  # last: not a noise vector
+    n = len(pairs)
+    fa = torch.full((n, Nt, L, L), 7.0, dtype=cdt, device=DEV)
+    fb = torch.full_like(fa, 7.0)
+    ops.bb_pair_fields(kind, eta.reshape(nrv, -1), g.reshape(nrv, -1), ep, pairs[:, 0].contiguous(),
+                       pairs[:, 1].contiguous(), L, fa, fb)
+    wa, wb = _fields_torch(kind, eta, g, ep, pairs[:-1, 0].long(), pairs[:-1, 1].long())
+    assert rel(fa[:-1].cpu(), wa.cpu()) < tol and rel(fb[:-1].cpu(), wb.cpu()) < tol
+    assert torch.count_nonzero(fa[-1]) == 0 and torch.count_nonzero(fb[-1]) == 0
+    A, B = torch.fft.ifft2(fa, norm="forward"), torch.fft.fft2(fb, norm="backward")
+    S = torch.zeros(L * L, dtype=torch.complex128, device=DEV)
+    ops.bb_kspace_acc(A, B, S)
+    ops.bb_kspace_acc(A, B, S)  # accumulates
+    want = 2 * (A.to(torch.complex128) * B.to(torch.complex128)).sum(dim=(0, 1)).reshape(-1)
+    assert rel(S.cpu(), want.cpu()) < 1e-12
