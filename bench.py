@@ -37,7 +37,7 @@ UNIT = "trajectories/hour"
 # workload, mixed precision, 2 right-hand sides: ncu --metrics
 # dram__bytes_read.sum,dram__bytes_write.sum of `bench.py --solve-only 482`
 # (profiles/k_pcg_mixed_L48_Lt480_rhs2.md)
-PCG_DRAM_BYTES_PER_SITE_ITER = 71.1
+PCG_DRAM_BYTES_PER_SITE_ITER = 72.9
 # PCG iterations per solve of this workload (mixed, rtol 1e-10), as the GPU run
 # measures them; the CPU arms extrapolate a trajectory with it when they run alone
 CG_ITERS_PER_SOLVE = 482
@@ -600,6 +600,22 @@ def run_kernels(args):
         emit(f"k_boson_force ({prec})", f"{bs} fields", ms, bs * N * 2 * sp * 2)
         ms = timed(lambda: ops.boson_action(ang, L, 0.1, 10.0, momenta=ang))
         emit(f"k_boson_action ({prec})", f"{bs} fields with momenta", ms, bs * N * 2 * sp * 2)
+        # bond-bond correlator passes: 8 noise vectors, their 28 pairs
+        nrv = 8
+        eta_b = torch.randn((nrv, N), dtype=cdt, device=dev)
+        g_b = torch.randn((nrv, N), dtype=cdt, device=dev)
+        ep_b = torch.exp(1j * torch.rand(N, dtype=rdt, device=dev)).to(cdt)
+        prs = torch.combinations(torch.arange(nrv, device=dev), r=2).to(torch.int32)
+        ps_b, pt_b = prs[:, 0].contiguous(), prs[:, 1].contiguous()
+        fa_b = torch.empty((len(prs), Lt, L, L), dtype=cdt, device=dev)
+        fb_b = torch.empty_like(fa_b)
+        ms = timed(lambda: ops.bb_pair_fields("T21", eta_b, g_b, ep_b, ps_b, pt_b, L, fa_b, fb_b))
+        emit(f"k_bb_pair_fields (T21, {prec})", f"{len(prs)} pairs of {nrv} vectors", ms,
+             len(prs) * N * 2 * sv + (2 * nrv + 1) * N * sv)
+        S_b = torch.zeros(L * L, dtype=torch.complex128, device=dev)
+        ms = timed(lambda: ops.bb_kspace_acc(fa_b, fb_b, S_b))
+        emit(f"k_bb_kspace_acc ({prec})", f"{len(prs)} pairs x {Lt} slices", ms, len(prs) * N * 2 * sv)
+        del eta_b, g_b, fa_b, fb_b
         pm = torch.zeros_like(ang)
         fm = torch.ones_like(ang)
         dt = torch.full((bs,), 0.01, dtype=torch.float64, device=dev)

@@ -46,56 +46,70 @@ __device__ __forceinline__ Cx<R> conjc(Cx<R> a) {
   return mk<R>(a.re, -a.im);
 }
 
-// one thread per (pair, site of the chunk's slices); grid (sites / 256, pairs)
+// grid (pairs, slices), pairs the fast grid dimension: the blocks in flight
+// cover all pairs of a few slices, so each noise vector's values there come
+// from DRAM once and are reused from L2 by the other pairs.  A block walks the
+// sites of its slice without integer division.
 template <typename R>
 __global__ void __launch_bounds__(256) k_bb_pair_fields(BondArgs a) {
-  const int Vs = a.L * a.L;
+  const int L = a.L, Vs = L * L;
+  const int p = blockIdx.x, tau = blockIdx.y;
   const int64_t nsite = (int64_t)a.Nt * Vs;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nsite) return;
-  const int p = blockIdx.y;
   const int s = a.ps[p], t = a.pt[p];
-  const int64_t o = (int64_t)p * nsite + i;
+  R* fa = reinterpret_cast<R*>(a.fa) + 2 * ((int64_t)p * nsite + (int64_t)tau * Vs);
+  R* fb = reinterpret_cast<R*>(a.fb) + 2 * ((int64_t)p * nsite + (int64_t)tau * Vs);
   if ((unsigned)s >= (unsigned)a.nrv || (unsigned)t >= (unsigned)a.nrv) {  // not a noise vector: zero fields
-    *reinterpret_cast<Cx<R>*>(reinterpret_cast<R*>(a.fa) + 2 * o) = mk<R>(0, 0);
-    *reinterpret_cast<Cx<R>*>(reinterpret_cast<R*>(a.fb) + 2 * o) = mk<R>(0, 0);
+    for (int q = threadIdx.x; q < Vs; q += blockDim.x) {
+      reinterpret_cast<Cx<R>*>(fa)[q] = mk<R>(0, 0);
+      reinterpret_cast<Cx<R>*>(fb)[q] = mk<R>(0, 0);
+    }
     return;
   }
-  const int tau = (int)(i / Vs), site = (int)(i - (int64_t)tau * Vs);
-  const int y = site / a.L, x = site - y * a.L;
-  const int64_t r = i, r1 = (int64_t)tau * Vs + y * a.L + (x + 1 == a.L ? 0 : x + 1);
+  const int64_t sl = (int64_t)tau * Vs;
   const R* eta = reinterpret_cast<const R*>(a.eta);
   const R* g = reinterpret_cast<const R*>(a.g);
-  const int64_t os = (int64_t)s * nsite, ot = (int64_t)t * nsite;
-  const Cx<R> ep = ldcx(reinterpret_cast<const R*>(a.ep), r);
-  Cx<R> A, B;
-  if (a.kind == 1) {
-    // a = ec_s g_t(r+x) e,  b = g_s(r+x) ec_t e
-    A = cmul(cmul(conjc(ldcx(eta, os + r)), ldcx(g, ot + r1)), ep);
-    B = cmul(cmul(ldcx(g, os + r1), conjc(ldcx(eta, ot + r))), ep);
-  } else if (a.kind == 4) {
-    // a = ec_s(r+x) g_t e*,  b = g_s ec_t(r+x) e*
-    const Cx<R> em = conjc(ep);
-    A = cmul(cmul(conjc(ldcx(eta, os + r1)), ldcx(g, ot + r)), em);
-    B = cmul(cmul(ldcx(g, os + r), conjc(ldcx(eta, ot + r1))), em);
-  } else {
-    const Cx<R> ecs = conjc(ldcx(eta, os + r)), ecs1 = conjc(ldcx(eta, os + r1));
-    const Cx<R> ect = conjc(ldcx(eta, ot + r)), ect1 = conjc(ldcx(eta, ot + r1));
-    const Cx<R> gs = ldcx(g, os + r), gs1 = ldcx(g, os + r1);
-    const Cx<R> gt = ldcx(g, ot + r), gt1 = ldcx(g, ot + r1);
-    const R h = (R)0.5;
-    if (a.kind == 21) {
-      // a = (ec_s(r+x) g_t + ec_t(r+x) g_s) e* / 2,  b = (g_s(r+x) ec_t + g_t(r+x) ec_s) e / 2
-      A = h * cmul(cmul(ecs1, gt) + cmul(ect1, gs), conjc(ep));
-      B = h * cmul(cmul(gs1, ect) + cmul(gt1, ecs), ep);
+  const int64_t os = (int64_t)s * nsite + sl, ot = (int64_t)t * nsite + sl;
+  const R* epv = reinterpret_cast<const R*>(a.ep) + 2 * sl;
+  const int dx = blockDim.x % L, dy = blockDim.x / L;
+  int x = threadIdx.x % L, y = threadIdx.x / L;
+  for (int q = threadIdx.x; q < Vs; q += blockDim.x) {
+    const int r = q, r1 = y * L + (x + 1 == L ? 0 : x + 1);
+    const Cx<R> ep = ldcx(epv, r);
+    Cx<R> A, B;
+    if (a.kind == 1) {
+      // a = ec_s g_t(r+x) e,  b = g_s(r+x) ec_t e
+      A = cmul(cmul(conjc(ldcx(eta, os + r)), ldcx(g, ot + r1)), ep);
+      B = cmul(cmul(ldcx(g, os + r1), conjc(ldcx(eta, ot + r))), ep);
+    } else if (a.kind == 4) {
+      // a = ec_s(r+x) g_t e*,  b = g_s ec_t(r+x) e*
+      const Cx<R> em = conjc(ep);
+      A = cmul(cmul(conjc(ldcx(eta, os + r1)), ldcx(g, ot + r)), em);
+      B = cmul(cmul(ldcx(g, os + r), conjc(ldcx(eta, ot + r1))), em);
     } else {
-      // T2: a = (ec_s g_t(r+x) + ec_t g_s(r+x)) e / 2,  b = (g_s ec_t(r+x) + g_t ec_s(r+x)) e* / 2
-      A = h * cmul(cmul(ecs, gt1) + cmul(ect, gs1), ep);
-      B = h * cmul(cmul(gs, ect1) + cmul(gt, ecs1), conjc(ep));
+      const Cx<R> ecs = conjc(ldcx(eta, os + r)), ecs1 = conjc(ldcx(eta, os + r1));
+      const Cx<R> ect = conjc(ldcx(eta, ot + r)), ect1 = conjc(ldcx(eta, ot + r1));
+      const Cx<R> gs = ldcx(g, os + r), gs1 = ldcx(g, os + r1);
+      const Cx<R> gt = ldcx(g, ot + r), gt1 = ldcx(g, ot + r1);
+      const R h = (R)0.5;
+      if (a.kind == 21) {
+        // a = (ec_s(r+x) g_t + ec_t(r+x) g_s) e* / 2,  b = (g_s(r+x) ec_t + g_t(r+x) ec_s) e / 2
+        A = h * cmul(cmul(ecs1, gt) + cmul(ect1, gs), conjc(ep));
+        B = h * cmul(cmul(gs1, ect) + cmul(gt1, ecs), ep);
+      } else {
+        // T2: a = (ec_s g_t(r+x) + ec_t g_s(r+x)) e / 2,  b = (g_s ec_t(r+x) + g_t ec_s(r+x)) e* / 2
+        A = h * cmul(cmul(ecs, gt1) + cmul(ect, gs1), ep);
+        B = h * cmul(cmul(gs, ect1) + cmul(gt, ecs1), conjc(ep));
+      }
+    }
+    reinterpret_cast<Cx<R>*>(fa)[q] = A;
+    reinterpret_cast<Cx<R>*>(fb)[q] = B;
+    x += dx;
+    y += dy;
+    if (x >= L) {
+      x -= L;
+      ++y;
     }
   }
-  *reinterpret_cast<Cx<R>*>(reinterpret_cast<R*>(a.fa) + 2 * o) = A;
-  *reinterpret_cast<Cx<R>*>(reinterpret_cast<R*>(a.fb) + 2 * o) = B;
 }
 
 // S[k] += sum_i A[i][k] B[i][k] over n rows of Vs columns, in double.
@@ -135,9 +149,8 @@ int pair_fields_entry(int kind, const R* eta, const R* g, const R* ep, const int
                       int Nrv, int Lx, int Ltau, R* fa, R* fb, cudaStream_t st) {
   if (kind != 1 && kind != 21 && kind != 2 && kind != 4) return QEDF_ERR_ARG;
   if (!eta || !g || !ep || !ps || !pt || !fa || !fb) return QEDF_ERR_ARG;
-  if (npairs < 0 || npairs > 65535 || Lx < 1 || Ltau < 1 || Nrv < 2) return QEDF_ERR_ARG;
+  if (npairs < 0 || npairs > 65535 || Lx < 1 || Ltau < 1 || Ltau > 65535 || Nrv < 2) return QEDF_ERR_ARG;
   if (npairs == 0) return QEDF_OK;
-  const int64_t nsite = (int64_t)Ltau * Lx * Lx;
   BondArgs a;
   a.kind = kind;
   a.eta = eta;
@@ -151,7 +164,7 @@ int pair_fields_entry(int kind, const R* eta, const R* g, const R* ep, const int
   a.Nt = Ltau;
   a.fa = fa;
   a.fb = fb;
-  dim3 grid((unsigned)((nsite + 255) / 256), npairs);
+  dim3 grid(npairs, Ltau);
   k_bb_pair_fields<R><<<grid, 256, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
