@@ -42,6 +42,9 @@
 
 namespace qedf {
 
+// rows in flight per thread in the single-precision elementwise update
+constexpr int PCG_EW_STAGES = 4;
+
 __constant__ PreTable c_pre = {QEDF_PRE_LAYOUT, QEDF_PRE_EDGE_VALUES, QEDF_PRE_TAIL_VALUES,
                                QEDF_PRE_MIDDLE_VALUES, QEDF_PRE_CORNER_VALUES};
 static const PreTable h_pre = {QEDF_PRE_LAYOUT, QEDF_PRE_EDGE_VALUES, QEDF_PRE_TAIL_VALUES,
@@ -276,26 +279,30 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     double acc_a = 0, acc_b = 0, acc_c = 0;
     if (sizeof(RS) == 4 && kind == 1) {
       // The iteration update, single precision: the two input rows (Op, r)
-      // of this thread's next two rows are in flight while one row is
-      // updated, as 16-byte cp.async copies into a two-stage area behind the
-      // unit's r column (stage k & 1, [vector][thread] units).  A stage is
-      // refilled only after its values were used.
+      // of this thread's next PCG_EW_STAGES rows are in flight while one row
+      // is updated, as 16-byte cp.async copies into a staging area behind the
+      // unit's r column (stage k % PCG_EW_STAGES, [vector][thread] units).  A
+      // stage is refilled only after its values were used; every issue slot
+      // commits a group, empty past the last row, so that the wait count is
+      // a constant.
       uint4* stg = reinterpret_cast<uint4*>(dsm + ((size_t)Nt * CHC * sizeof(Cx<RS>) + 15) / 16 * 16);
       const int nthr = blockDim.x, t0 = tid / PPR;
       const int K = (jon && t0 < Nt) ? (Nt - 1 - t0) / rstep + 1 : 0;
       RS cpart = 0;  // this thread's |r|^2 in the iteration precision
       auto issue = [&](int k) {
-        const int64_t i2 = 2 * (base + (int64_t)(t0 + k * rstep) * Vs + c0 + 2 * j);
-        uint4* d = stg + (size_t)(k & 1) * 2 * nthr + tid;
-        cp_async16(d, opv + i2);
-        cp_async16(d + nthr, r + i2);
+        if (k < K) {
+          const int64_t i2 = 2 * (base + (int64_t)(t0 + k * rstep) * Vs + c0 + 2 * j);
+          uint4* d = stg + (size_t)(k % PCG_EW_STAGES) * 2 * nthr + tid;
+          cp_async16(d, opv + i2);
+          cp_async16(d + nthr, r + i2);
+        }
         cp_async_commit();
       };
-      if (K > 0) issue(0);
-      if (K > 1) issue(1);
+#pragma unroll
+      for (int k = 0; k < PCG_EW_STAGES; ++k) issue(k);
       for (int k = 0; k < K; ++k) {
-        if (k + 1 < K) cp_async_wait<1>(); else cp_async_wait<0>();
-        const RS* d = reinterpret_cast<const RS*>(stg + (size_t)(k & 1) * 2 * nthr + tid);
+        cp_async_wait<PCG_EW_STAGES - 1>();
+        const RS* d = reinterpret_cast<const RS*>(stg + (size_t)(k % PCG_EW_STAGES) * 2 * nthr + tid);
         Cx<RS> o0, o1, r0, r1;
         ld2c(d, o0, o1);
         ld2c(d + 4 * nthr, r0, r1);
@@ -306,8 +313,9 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         st2(r + i2, r0, r1);
         cpart = fma(r0.re, r0.re, fma(r0.im, r0.im, fma(r1.re, r1.re, fma(r1.im, r1.im, cpart))));
         st2(reinterpret_cast<RS*>(rsm + t * CHC + 2 * j), r0, r1);
-        if (k + 2 < K) issue(k + 2);
+        issue(k + PCG_EW_STAGES);
       }
+      cp_async_wait<0>();
       acc_c += (double)cpart;
     } else
 #pragma unroll 2
@@ -944,10 +952,10 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   const int threads = std::min(MaxT<BY, ECS>::value, std::max(128, eng_threads));
   size_t smem = slice_smem_bytes<RS, ECS>(Lmax, BY, 2);
   smem = std::max(smem, slice_smem_bytes<RH, ECH>(Lmax, BY, 2));
-  // elementwise units: the r column, and in single precision the two-stage
+  // elementwise units: the r column, and in single precision the staging
   // area of the update pass
   smem = std::max(smem, ((sizeof(Cx<RS>) * (size_t)Ntmax * PCG_CHUNK + 15) / 16 * 16) +
-                            (sizeof(RS) == 4 ? 2 * 2 * 16 * (size_t)threads : 0));
+                            (sizeof(RS) == 4 ? PCG_EW_STAGES * 2 * 16 * (size_t)threads : 0));
   if (smem + sizeof(RhsState) > 227 * 1024) return QEDF_ERR_SIZE;
   auto kern = k_pcg<RS, RH, A, BY, ECS, ECH>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
