@@ -53,28 +53,31 @@ static const PreTable h_pre = {QEDF_PRE_LAYOUT, QEDF_PRE_EDGE_VALUES, QEDF_PRE_T
 // ---------------------------------------------------------------------------
 // bounded grid barrier
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, long long budget) {
+// bar[0] counts arrivals over the whole solve (zeroed per solve); barrier n
+// of a block is passed once the count reaches n * nblocks.  Arrival is a
+// release reduction without a reply, and waiting an acquire load of the
+// count, so the last block's arrival ends the barrier directly.  bar[2] is
+// the error word.  `target` is the calling block's count to wait for, kept
+// by its thread 0 across calls.
+__device__ __forceinline__ bool grid_barrier(unsigned int* bar, unsigned int nblocks, long long budget,
+                                             unsigned int& target) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int* gen = bar + 1;
     volatile unsigned int* err = bar + 2;
-    const unsigned int g = *gen;
+    target += nblocks;
     __threadfence();
-    const unsigned int arrived = atomicAdd(bar, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      const long long t0 = clock64();
-      while (*gen == g) {
-        if (*err) break;
-        if (clock64() - t0 > budget) {
-          atomicExch(bar + 2, (unsigned int)QEDF_ERR_TIMEOUT);
-          break;
-        }
-        __nanosleep(64);
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;\n" ::"l"(bar), "r"(1u) : "memory");
+    const long long t0 = clock64();
+    while (true) {
+      unsigned int v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(bar) : "memory");
+      if ((int)(v - target) >= 0) break;
+      if (*err) break;
+      if (clock64() - t0 > budget) {
+        atomicExch(bar + 2, (unsigned int)QEDF_ERR_TIMEOUT);
+        break;
       }
+      __nanosleep(32);
     }
     __threadfence();
   }
@@ -641,13 +644,14 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
 
   // ---------------------------------------------------------------------------
   const long long budget = p.timeout_cycles;
+  unsigned int bar_target = 0;  // grid barrier count to wait for (thread 0)
   bool ok = true;
   PhaseClock pc(p.prof);
   const long long t_begin = pc.prof ? clock64() : 0;
 
   // init: x = 0, r = b, z = P r
   for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) elementwise(0, u, 0);
-  ok = grid_barrier(p.bar, nblk, budget);
+  ok = grid_barrier(p.bar, nblk, budget, bar_target);
   pc.lap(0);
   int slot = 0;  // accumulator slot holding the current rr / rz
   if (ok) {
@@ -701,19 +705,19 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
           acc.ru_rz[v] = 0;
         }
       for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) fold_unit(u, false);
-      if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+      if (!(ok = grid_barrier(p.bar, nblk, budget, bar_target))) break;
       for (int u = blockIdx.x; u < p.unitsA; u += gridDim.x) {
         const int s = find_sys_A(p, u);
         const int v = p.sys[s].rhs0 + (u - p.sys[s].unitA0) / p.sys[s].nslab;
         if (st.ru[v]) operator_unit_true_residual(u);
       }
-      if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+      if (!(ok = grid_barrier(p.bar, nblk, budget, bar_target))) break;
       for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) {
         int s, v, c0, c1;
         unitE(u, s, v, c0, c1);
         if (st.ru[v]) elementwise(2, u, 0);
       }
-      if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+      if (!(ok = grid_barrier(p.bar, nblk, budget, bar_target))) break;
       for (int v = tid; v < NV; v += blockDim.x) {
         if (!st.ru[v]) continue;
         st.pending[v] = 0;  // folded into x above
@@ -754,7 +758,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         acc.rz[(slot ^ 1) * NV + v] = 0;
       }
     pc.lap(1);
-    if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+    if (!(ok = grid_barrier(p.bar, nblk, budget, bar_target))) break;
     pc.lap(2);
 
     // ---- phase BC
@@ -771,7 +775,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     if (blockIdx.x == 0)  // pAp slot of the next iteration
       for (int v = tid; v < NV; v += blockDim.x) acc.pAp[(aslot ^ 1) * NV + v] = 0;
     pc.lap(3);
-    if (!(ok = grid_barrier(p.bar, nblk, budget))) break;
+    if (!(ok = grid_barrier(p.bar, nblk, budget, bar_target))) break;
     pc.lap(4);
     slot ^= 1;
     for (int v = tid; v < NV; v += blockDim.x) {
