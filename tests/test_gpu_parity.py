@@ -288,8 +288,11 @@ def test_pcg_solves(mode, L, Nt, bs, kind):
     assert relerr(x, xo) < (1e-3 if mode == "fp32" else 1e-7)
 
 
-def test_pcg_batch_of_uneven_lattices():
-    """Several lattices of different L and Ltau in one launch, each with its own mask."""
+@pytest.mark.parametrize("mode", ["mixed", "fp64"])
+def test_pcg_batch_of_uneven_lattices(mode):
+    """Several lattices of different L and Ltau in one launch, each with its own mask.  In the
+    plain mode the systems that stop early still carry their last x update, which the solve
+    applies at its end."""
     from qed_fermion_b200.solver import PcgSolver, System
     systems = [System(4, 30, 2), System(6, 40, 1), System(4, 12, 1), System(8, 26, 3, True)]
     phis, bs_, refs = [], [], []
@@ -300,8 +303,8 @@ def test_pcg_batch_of_uneven_lattices():
         phis.append(phi.reshape(-1))
         bs_.append(b.reshape(-1))
         refs.append((s, phi, b))
-    solver = PcgSolver(systems, mode="mixed", rtol=1e-10, max_iter=20000, device=DEV)
-    res = solver.solve(torch.tensor(np.concatenate(phis), dtype=torch.float32, device=DEV),
+    solver = PcgSolver(systems, mode=mode, rtol=1e-10, max_iter=20000, device=DEV)
+    res = solver.solve(torch.tensor(np.concatenate(phis), dtype=solver.angle_dtype, device=DEV),
                        torch.tensor(np.concatenate(bs_), device=DEV))
     assert res.status.cpu().tolist() == [0] * solver.nrhs
     x = res.x.cpu().numpy()
@@ -310,13 +313,34 @@ def test_pcg_batch_of_uneven_lattices():
         n = s.n * s.nrhs
         xs = x[off:off + n].reshape(s.nrhs, s.Ltau, s.Lx * s.Lx)
         off += n
-        ph = phi.astype(np.float32).astype(np.float64)
+        ph = phi.astype(np.float32).astype(np.float64) if mode == "mixed" else phi
         if s.shared_boson:
             ph = np.repeat(ph, s.nrhs, axis=0)
         r = b - O.mhm_vec(ph, xs, s.Lx, 0.1).reshape(s.nrhs, -1)
         assert np.all(np.linalg.norm(r, axis=1) / np.linalg.norm(b, axis=1) < 2e-10)
     its = res.iters.cpu().tolist()
     assert len(set(its)) > 1  # the masks stopped the systems at different iterations
+
+
+@pytest.mark.parametrize("mode,tol", [("fp64", 1e-11), ("mixed", 2e-5), ("fp32", 2e-5)])
+@pytest.mark.parametrize("iters", [1, 4, 9])
+def test_pcg_truncated_solves_match_oracle_iterates(mode, tol, iters):
+    """Solves cut off after a few iterations (rtol unreachable) against the oracle's iterate
+    after the same number of iterations: the last iteration's x update, which the kernel
+    applies in the next operator pass, is applied at the end of the solve."""
+    from qed_fermion_b200.solver import PcgSolver, System
+    L, Nt, bs = 4, 30, 2
+    boson, b = rand_case(L, Nt, bs, seed=77, kind="piflux")
+    phi = O.ref_to_kernel_layout(boson)
+    solver = PcgSolver([System(L, Nt, bs)], mode=mode, rtol=1e-15, max_iter=iters, device=DEV)
+    res = solver.solve(torch.tensor(phi.reshape(bs, -1), dtype=solver.angle_dtype, device=DEV),
+                       torch.tensor(b, dtype=solver.vec_dtype, device=DEV))
+    assert res.iters.cpu().tolist() == [iters] * bs
+    phi_used = phi.astype(np.float32).astype(np.float64) if solver.angle_dtype == torch.float32 else phi
+    A = lambda v: O.mhm_vec(phi_used, v.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    Pf = lambda v: O.precon_vec(v.reshape(bs, Nt, L * L), O.precon_tau_matrix(Nt)).reshape(bs, -1)
+    xo, _, _ = O.pcg_batched_masked(A, b, Pf, 1e-15, iters, reference_alias=False)
+    assert relerr(res.x.cpu().numpy().reshape(bs, -1), xo) < tol
 
 
 def test_pcg_status_codes():
