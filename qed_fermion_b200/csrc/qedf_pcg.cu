@@ -819,6 +819,27 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
 // ---------------------------------------------------------------------------
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Slab length of the operator units: units are dealt to the blocks in turn,
+// so the busiest block runs ceil(units / nblk) units of T slices plus one
+// halo slice each.  The T that minimises that count wins (the longer T on
+// ties: fewer units, fewer per-unit reductions).
+static int auto_slab(const qedf_system* sys, int nsys, int nblk) {
+  int ntmax = 1;
+  for (int k = 0; k < nsys; ++k) ntmax = std::max(ntmax, sys[k].Ltau);
+  int best = ntmax;
+  long long best_cost = -1;
+  for (int T = ntmax; T >= 1; --T) {
+    long long units = 0;
+    for (int k = 0; k < nsys; ++k) units += (long long)sys[k].nrhs * ((sys[k].Ltau + T - 1) / T);
+    const long long cost = (units + nblk - 1) / nblk * (T + 1);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = T;
+    }
+  }
+  return best;
+}
+
 int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts* o) {
   std::memset(&p, 0, sizeof(p));
   if (!sys || !o || nsys <= 0 || nsys > PCG_MAX_SYS) return QEDF_ERR_ARG;
@@ -841,15 +862,7 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
     S.nrhs = q.nrhs;
     S.shared = q.shared_boson ? 1 : 0;
     S.precon = (o->use_precon && q.Ltau >= PRE_MIN_LTAU) ? 1 : 0;
-    if (o->slab > 0) {
-      S.T = o->slab;
-    } else {
-      // about one operator unit per block over all right-hand sides
-      int total_rhs = 0;
-      for (int k = 0; k < nsys; ++k) total_rhs += sys[k].nrhs;
-      const int per_rhs = std::max(1, nblk / std::max(1, total_rhs));
-      S.T = std::max(1, (q.Ltau + per_rhs - 1) / per_rhs);
-    }
+    S.T = o->slab > 0 ? o->slab : auto_slab(sys, nsys, nblk);
     // the preconditioner rows that are the bulk band (middle values at every
     // distance, nothing else): one contiguous range away from both tau ends
     S.pmid_lo = S.pmid_hi = 0;
