@@ -167,10 +167,13 @@ def bb_pair_fields(kind: str, eta: torch.Tensor, g_eta: torch.Tensor, ephase: to
             raise RuntimeError("bb_pair_fields: complex tensors must share eta's dtype and be contiguous")
     if ps.dtype != torch.int32 or pt.dtype != torch.int32 or not ps.is_contiguous() or not pt.is_contiguous():
         raise RuntimeError("bb_pair_fields: pair indices must be contiguous int32")
+    if eta.dim() != 2:
+        raise RuntimeError("bb_pair_fields: eta must be [Nrv, Ltau * Lx^2]")
     nrv, N = eta.shape
     Vs, Ltau = lattice_dims(N, Lx)
     npairs = ps.numel()
-    if fa.numel() < npairs * N or fb.numel() < npairs * N or ephase.numel() != N or pt.numel() != npairs:
+    if (g_eta.numel() != eta.numel() or fa.numel() < npairs * N or fb.numel() < npairs * N
+            or ephase.numel() != N or pt.numel() != npairs):
         raise RuntimeError("bb_pair_fields: buffer sizes do not match")
     _lib.call(f"qedf_bb_pair_fields_{prec}", BB_KINDS[kind], ptr(eta), ptr(g_eta), ptr(ephase), ptr(ps), ptr(pt),
               npairs, nrv, Lx, Ltau, ptr(fa), ptr(fb), stream_handle())
