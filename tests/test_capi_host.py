@@ -53,6 +53,18 @@ def test_host_validation_rejects_before_launch():
     assert lib.qedf_mhm_vec_c64(p, p, q, 1, 80, 10, 0.1, 1, 0, 0, None) == _lib.QEDF_ERR_SIZE
     # L = 66 needs 2 x 6 tiles; asking for 2 x 2 is an argument error
     assert lib.qedf_mhm_vec_c64(p, p, q, 1, 66, 10, 0.1, 1, 2, 0, None) == _lib.QEDF_ERR_ARG
+    # correlator passes: unknown kind, null pointers, too many pairs or slices, one noise
+    # vector, negative row count
+    bb = lib.qedf_bb_pair_fields_c64
+    assert bb(3, p, p, p, p, p, 1, 4, 4, 10, p, q, None) == _lib.QEDF_ERR_ARG
+    assert bb(1, None, p, p, p, p, 1, 4, 4, 10, p, q, None) == _lib.QEDF_ERR_ARG
+    assert bb(21, p, p, p, p, p, 70000, 4, 4, 10, p, q, None) == _lib.QEDF_ERR_ARG
+    assert lib.qedf_bb_pair_fields_c128(2, p, p, p, p, p, 1, 4, 4, 70000, p, q, None) == _lib.QEDF_ERR_ARG
+    assert bb(4, p, p, p, p, p, 1, 1, 4, 10, p, q, None) == _lib.QEDF_ERR_ARG
+    assert bb(1, p, p, p, p, p, 0, 4, 4, 10, p, q, None) == _lib.QEDF_OK  # nothing to do
+    assert lib.qedf_bb_kspace_acc_c64(p, p, -1, 16, p, None) == _lib.QEDF_ERR_ARG
+    assert lib.qedf_bb_kspace_acc_c128(p, None, 4, 16, p, None) == _lib.QEDF_ERR_ARG
+    assert lib.qedf_bb_kspace_acc_c128(p, p, 0, 16, p, None) == _lib.QEDF_OK  # nothing to do
 
 
 def test_pcg_workspace_query():
