@@ -45,6 +45,7 @@ class QedfPcgOpts(ctypes.Structure):
         ("chunk", c_int),
         ("timeout_ms", c_double),
         ("profile", c_void_p),
+        ("l2_persist", c_int),
     ]
 
 

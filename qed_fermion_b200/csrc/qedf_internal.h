@@ -109,6 +109,7 @@ struct PcgParams {
   PcgSys sys[PCG_MAX_SYS];
   int mode;  // QEDF_PCG_PLAIN_F32, QEDF_PCG_PLAIN_F64, QEDF_PCG_MIXED
   int xs;    // allow the warp-shuffle engine for the single-precision iterations
+  int l2;    // 0: L2 persisting window over the iteration vectors when they fit; -1: off
   int max_iter, ru_interval;
   double rtol, ru_delta;
   double c1, ch, t1, th, Cb;

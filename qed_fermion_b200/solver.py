@@ -56,12 +56,18 @@ class PcgSolver:
     The device workspace is one torch allocation made here; ``solve`` itself
     allocates only its outputs (or none, given ``out``) and never synchronises
     the host, so it can be captured in a CUDA graph.
+
+    ``l2_persist`` (default on) keeps the iteration vectors in the L2
+    persisting set-aside when they fit; it raises the process's
+    ``cudaLimitPersistingL2CacheSize`` to their size on the first solve (not
+    during a graph capture).  Pass False to leave L2 policy alone.
     """
 
     def __init__(self, systems: Sequence[System], mode: str = "mixed", rtol: float = 1e-10,
                  max_iter: int = 10000, dtau: float = 0.1, use_precon: bool = True,
                  ru_interval: int = 50, ru_delta: float = 0.1, by: int = 0, slab: int = 0,
-                 chunk: int = 0, timeout_ms: float = 2000.0, profile: bool = False, device=None):
+                 chunk: int = 0, timeout_ms: float = 2000.0, profile: bool = False, device=None,
+                 l2_persist: bool = True):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {sorted(MODES)}")
         self.systems = [s if isinstance(s, System) else System(*s) for s in systems]
@@ -75,7 +81,8 @@ class PcgSolver:
         self._opts = _lib.QedfPcgOpts(MODES[mode], int(max_iter), float(rtol), float(dtau),
                                       1 if use_precon else 0, int(ru_interval), float(ru_delta), int(by),
                                       int(slab), int(chunk), float(timeout_ms),
-                                      self.profile.data_ptr() if profile else None)
+                                      self.profile.data_ptr() if profile else None,
+                                      0 if l2_persist else -1)
         nbytes = _lib.load().qedf_pcg_workspace_bytes(self._sys, n, self._opts)
         if nbytes < 0:
             raise ValueError("invalid system description for the PCG solver")

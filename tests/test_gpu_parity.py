@@ -343,6 +343,24 @@ def test_pcg_truncated_solves_match_oracle_iterates(mode, tol, iters):
     assert relerr(res.x.cpu().numpy().reshape(bs, -1), xo) < tol
 
 
+def test_pcg_l2_window_changes_no_result():
+    """The L2 persisting window is a cache policy only: solves with and without it agree bit
+    for bit."""
+    from qed_fermion_b200.solver import PcgSolver, System
+    L, Nt, bs = 6, 40, 2
+    boson, b = rand_case(L, Nt, bs, seed=5, kind="piflux")
+    phi = O.ref_to_kernel_layout(boson)
+    xs = []
+    for on in (True, False):
+        solver = PcgSolver([System(L, Nt, bs)], mode="mixed", rtol=1e-10, max_iter=5000, device=DEV,
+                           l2_persist=on)
+        res = solver.solve(torch.tensor(phi.reshape(bs, -1), dtype=torch.float32, device=DEV),
+                           torch.tensor(b, device=DEV))
+        assert res.status.cpu().tolist() == [0] * bs
+        xs.append(res.x.clone())
+    assert torch.equal(xs[0], xs[1])
+
+
 def test_pcg_status_codes():
     from qed_fermion_b200 import _lib
     from qed_fermion_b200.solver import PcgSolver, System
