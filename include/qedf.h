@@ -209,10 +209,11 @@ typedef struct {
                          accumulate SM clock cycles of block 0: 0 init, 1 operator phases,
                          2 waits after them, 3 elementwise phases, 4 waits after them,
                          5 reliable updates, 6 per-iteration bookkeeping, 7 whole solve */
-  int l2_persist;     /* 0 (default): keep the iteration vectors p, z and M^dag M p in the L2
-                         persisting set-aside when they fit, raising the context's
-                         cudaLimitPersistingL2CacheSize to their size if it is lower (never
-                         while the stream is capturing); -1: leave L2 policy alone */
+  int l2_persist;     /* 0 (default): an L2 access-policy window over the iteration vectors
+                         p, z and M^dag M p, fitted to the context's persisting set-aside as
+                         it is (cudaLimitPersistingL2CacheSize is never changed), released
+                         to normal status after the solve by one small kernel;
+                         -1: no window and no extra kernel */
 } qedf_pcg_opts;
 
 /* Bytes of device workspace qedf_pcg_solve needs for these systems. */

@@ -118,8 +118,13 @@ def call(name, *args):
     lib = load()
     st = getattr(lib, name)(*args)
     if name not in _HOST_ONLY:
-        # qedf_pcg_solve launches a small preparation kernel and the solver
-        LAUNCHES["count"] += 2 if name.startswith("qedf_pcg_solve") else 1
+        # qedf_pcg_solve launches a small preparation kernel, the solver and,
+        # unless l2_persist is -1, the kernel that releases the L2 window
+        if name.startswith("qedf_pcg_solve"):
+            opts = next((a for a in args if isinstance(a, QedfPcgOpts)), None)
+            LAUNCHES["count"] += 2 if (opts is not None and opts.l2_persist < 0) else 3
+        else:
+            LAUNCHES["count"] += 1
     if st != QEDF_OK:
         raise QedfError(name, st, lib.qedf_status_string(st).decode())
     return st

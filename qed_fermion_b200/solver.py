@@ -57,10 +57,10 @@ class PcgSolver:
     allocates only its outputs (or none, given ``out``) and never synchronises
     the host, so it can be captured in a CUDA graph.
 
-    ``l2_persist`` (default on) keeps the iteration vectors in the L2
-    persisting set-aside when they fit; it raises the process's
-    ``cudaLimitPersistingL2CacheSize`` to their size on the first solve (not
-    during a graph capture).  Pass False to leave L2 policy alone.
+    ``l2_persist`` (default on) gives the solver launch an L2 access-policy
+    window over its iteration vectors, fitted to the process's persisting
+    set-aside as it is (the limit is never changed), and releases the window's
+    lines after the solve.  Pass False for no window.
     """
 
     def __init__(self, systems: Sequence[System], mode: str = "mixed", rtol: float = 1e-10,
