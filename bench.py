@@ -37,7 +37,7 @@ UNIT = "trajectories/hour"
 # workload, mixed precision, 2 right-hand sides: ncu --metrics
 # dram__bytes_read.sum,dram__bytes_write.sum of `bench.py --solve-only 482`
 # (profiles/k_pcg_mixed_L48_Lt480_rhs2.md)
-PCG_DRAM_BYTES_PER_SITE_ITER = 72.9
+PCG_DRAM_BYTES_PER_SITE_ITER = 72.7
 # PCG iterations per solve of this workload (mixed, rtol 1e-10), as the GPU run
 # measures them; the CPU arms extrapolate a trajectory with it when they run alone
 CG_ITERS_PER_SOLVE = 482
