@@ -981,15 +981,13 @@ __global__ void k_l2_release(const uint4* base, size_t n16) {
 
 static bool pcg_l2_window(const PcgParams& p, cudaLaunchAttribute& at) {
   if (p.l2 < 0) return false;
-  int dev = 0, maxp = 0, maxw = 0;
+  int dev = 0, maxw = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
       cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
   const size_t vecb = (size_t)(static_cast<const char*>(p.p1) - static_cast<const char*>(p.p0));
-  (void)maxp;
   const size_t maxwin = (size_t)std::max(maxw, 0);
   void* base = p.p0;
   size_t bytes = 4 * vecb;  // p0, p1, z, Op
