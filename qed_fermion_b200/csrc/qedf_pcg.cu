@@ -4,13 +4,18 @@
 // grid-wide phases separated by grid barriers:
 //
 //   A  (operator units: one right-hand side x one tau-slab)
+//        x    += alpha_old p_old          (the previous iteration's update,
+//                                          on the slab's own slices)
 //        p_new = z + beta p_old          (halo slices recomputed, not exchanged)
 //        Op    = M^dag M p_new            (slice engine, registers + smem)
 //        pAp  += Re p_new^dag Op          (double)
 //   BC (elementwise units: one right-hand side x a chunk of sites, all tau)
-//        x += alpha p_new,  r -= alpha Op
+//        r -= alpha Op
 //        z  = (P_tau (x) I) r             (the chunk's r column stays in smem)
 //        rr += |r|^2,  rz += Re r^dag z   (double)
+//
+// The last iteration's x update is applied by a reliable update's fold or at
+// the end of the solve.
 //
 // which is the arithmetic of preconditioned_cg_fast_test
 // (hmc_sampler_batch.py:751-846) with the reference's per-iteration torch
