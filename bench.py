@@ -708,6 +708,30 @@ def run_configs(args):
     ms, _ = timed(lambda: se.get_bond_bond_per_b2(bos))
     emit({"config": "C4a", "what": "bond-bond correlators T1+T21+T2+T4+Tvv over the 2016 noise pairs "
                                    "(complex128, cuFFT)", "ms": ms})
+    # where one correlator's time goes: the passes of one chunk of pairs (the
+    # default 1 GiB chunk: 34 pairs), each timed over 10 launches
+    e128 = se.eta.to(torch.complex128).resolve_conj().contiguous()
+    g128 = se.G_eta.to(torch.complex128).resolve_conj().contiguous()
+    ep = torch.exp(1j * bos.permute(0, 1, 4, 3, 2)[0, 0].to(torch.float64)).contiguous()
+    prs = torch.combinations(torch.arange(nrv, device=dev), r=2).to(torch.int32)
+    nch = (1 << 30) // (4 * L * L * Lt * 16)
+    ps, pt = prs[:nch, 0].contiguous(), prs[:nch, 1].contiguous()
+    fa = torch.empty((nch, Lt, L, L), dtype=torch.complex128, device=dev)
+    fb = torch.empty_like(fa)
+    Sk = torch.zeros(L * L, dtype=torch.complex128, device=dev)
+    chunks = len(prs) / nch
+    parts = {}
+    parts["pair_fields"], _ = timed(lambda: ops.bb_pair_fields("T21", e128, g128, ep, ps, pt, L, fa, fb), reps=10)
+    parts["ifft2"], A = timed(lambda: torch.fft.ifft2(fa, norm="forward"), reps=10)
+    parts["fft2"], B = timed(lambda: torch.fft.fft2(fb, norm="backward"), reps=10)
+    parts["kspace_acc"], _ = timed(lambda: ops.bb_kspace_acc(A, B, Sk), reps=10)
+    field_gb = nch * L * L * Lt * 16 / 1e9
+    emit({"config": "C4a", "what": f"one correlator (T21) per chunk of {nch} pairs, {chunks:.1f} chunks",
+          "ms_per_chunk": parts, "ms_per_correlator": {k: v * chunks for k, v in parts.items()},
+          "GBps": {"pair_fields": 2 * field_gb / (parts["pair_fields"] / 1e3),
+                   "ifft2": 2 * field_gb / (parts["ifft2"] / 1e3), "fft2": 2 * field_gb / (parts["fft2"] / 1e3),
+                   "kspace_acc": 2 * field_gb / (parts["kspace_acc"] / 1e3)}})
+    del fa, fb, A, B
 
     # C4b: 16 lattices L in {12, 18, 24, 30} x 4, Ltau = 10 L, one launch
     Ls = [12, 18, 24, 30] * 4
