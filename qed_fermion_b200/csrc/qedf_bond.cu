@@ -46,63 +46,77 @@ __device__ __forceinline__ Cx<R> conjc(Cx<R> a) {
   return mk<R>(a.re, -a.im);
 }
 
-// grid (pairs, slices), pairs the fast grid dimension: the blocks in flight
-// cover all pairs of a few slices, so each noise vector's values there come
-// from DRAM once and are reused from L2 by the other pairs.  A block walks the
-// sites of its slice without integer division.
+// grid (groups of BB_GROUP consecutive pairs, slices), the group index the
+// fast grid dimension: the blocks in flight cover all pairs of a few slices,
+// so each noise vector's values there come from DRAM once.  Within a block
+// the pairs are the inner loop of each site: e^{i phi} is read once per
+// site, and the first vector's values once per run of pairs that share it
+// (in torch.combinations order most consecutive pairs do), which halves the
+// L2 reads of T21 and T2.  Sites are walked without integer division.
+constexpr int BB_GROUP = 8;
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_bb_pair_fields(BondArgs a) {
   const int L = a.L, Vs = L * L;
-  const int p = blockIdx.x, tau = blockIdx.y;
+  const int p0 = blockIdx.x * BB_GROUP, tau = blockIdx.y;
+  const int np = min(BB_GROUP, a.npairs - p0);
   const int64_t nsite = (int64_t)a.Nt * Vs;
-  const int s = a.ps[p], t = a.pt[p];
-  R* fa = reinterpret_cast<R*>(a.fa) + 2 * ((int64_t)p * nsite + (int64_t)tau * Vs);
-  R* fb = reinterpret_cast<R*>(a.fb) + 2 * ((int64_t)p * nsite + (int64_t)tau * Vs);
-  if ((unsigned)s >= (unsigned)a.nrv || (unsigned)t >= (unsigned)a.nrv) {  // not a noise vector: zero fields
-    for (int q = threadIdx.x; q < Vs; q += blockDim.x) {
-      reinterpret_cast<Cx<R>*>(fa)[q] = mk<R>(0, 0);
-      reinterpret_cast<Cx<R>*>(fb)[q] = mk<R>(0, 0);
-    }
-    return;
-  }
   const int64_t sl = (int64_t)tau * Vs;
   const R* eta = reinterpret_cast<const R*>(a.eta);
   const R* g = reinterpret_cast<const R*>(a.g);
-  const int64_t os = (int64_t)s * nsite + sl, ot = (int64_t)t * nsite + sl;
   const R* epv = reinterpret_cast<const R*>(a.ep) + 2 * sl;
   const int dx = blockDim.x % L, dy = blockDim.x / L;
   int x = threadIdx.x % L, y = threadIdx.x / L;
   for (int q = threadIdx.x; q < Vs; q += blockDim.x) {
     const int r = q, r1 = y * L + (x + 1 == L ? 0 : x + 1);
     const Cx<R> ep = ldcx(epv, r);
-    Cx<R> A, B;
-    if (a.kind == 1) {
-      // a = ec_s g_t(r+x) e,  b = g_s(r+x) ec_t e
-      A = cmul(cmul(conjc(ldcx(eta, os + r)), ldcx(g, ot + r1)), ep);
-      B = cmul(cmul(ldcx(g, os + r1), conjc(ldcx(eta, ot + r))), ep);
-    } else if (a.kind == 4) {
-      // a = ec_s(r+x) g_t e*,  b = g_s ec_t(r+x) e*
-      const Cx<R> em = conjc(ep);
-      A = cmul(cmul(conjc(ldcx(eta, os + r1)), ldcx(g, ot + r)), em);
-      B = cmul(cmul(ldcx(g, os + r), conjc(ldcx(eta, ot + r1))), em);
-    } else {
-      const Cx<R> ecs = conjc(ldcx(eta, os + r)), ecs1 = conjc(ldcx(eta, os + r1));
-      const Cx<R> ect = conjc(ldcx(eta, ot + r)), ect1 = conjc(ldcx(eta, ot + r1));
-      const Cx<R> gs = ldcx(g, os + r), gs1 = ldcx(g, os + r1);
-      const Cx<R> gt = ldcx(g, ot + r), gt1 = ldcx(g, ot + r1);
-      const R h = (R)0.5;
-      if (a.kind == 21) {
-        // a = (ec_s(r+x) g_t + ec_t(r+x) g_s) e* / 2,  b = (g_s(r+x) ec_t + g_t(r+x) ec_s) e / 2
-        A = h * cmul(cmul(ecs1, gt) + cmul(ect1, gs), conjc(ep));
-        B = h * cmul(cmul(gs1, ect) + cmul(gt1, ecs), ep);
-      } else {
-        // T2: a = (ec_s g_t(r+x) + ec_t g_s(r+x)) e / 2,  b = (g_s ec_t(r+x) + g_t ec_s(r+x)) e* / 2
-        A = h * cmul(cmul(ecs, gt1) + cmul(ect, gs1), ep);
-        B = h * cmul(cmul(gs, ect1) + cmul(gt, ecs1), conjc(ep));
+    const Cx<R> em = conjc(ep);
+    int s_prev = -1;
+    Cx<R> ecs = mk<R>(0, 0), ecs1 = ecs, gs = ecs, gs1 = ecs;
+    for (int k = 0; k < np; ++k) {
+      const int p = p0 + k;
+      const int s = a.ps[p], t = a.pt[p];
+      Cx<R>* fa = reinterpret_cast<Cx<R>*>(a.fa) + (int64_t)p * nsite + sl;
+      Cx<R>* fb = reinterpret_cast<Cx<R>*>(a.fb) + (int64_t)p * nsite + sl;
+      if ((unsigned)s >= (unsigned)a.nrv || (unsigned)t >= (unsigned)a.nrv) {  // not a noise vector: zero
+        fa[q] = mk<R>(0, 0);
+        fb[q] = mk<R>(0, 0);
+        continue;
       }
+      const int64_t os = (int64_t)s * nsite + sl, ot = (int64_t)t * nsite + sl;
+      if (s != s_prev) {  // the first vector's values at r and r + x
+        ecs = conjc(ldcx(eta, os + r));
+        ecs1 = conjc(ldcx(eta, os + r1));
+        gs = ldcx(g, os + r);
+        gs1 = ldcx(g, os + r1);
+        s_prev = s;
+      }
+      Cx<R> A, B;
+      if (a.kind == 1) {
+        // a = ec_s g_t(r+x) e,  b = g_s(r+x) ec_t e
+        A = cmul(cmul(ecs, ldcx(g, ot + r1)), ep);
+        B = cmul(cmul(gs1, conjc(ldcx(eta, ot + r))), ep);
+      } else if (a.kind == 4) {
+        // a = ec_s(r+x) g_t e*,  b = g_s ec_t(r+x) e*
+        A = cmul(cmul(ecs1, ldcx(g, ot + r)), em);
+        B = cmul(cmul(gs, conjc(ldcx(eta, ot + r1))), em);
+      } else {
+        const Cx<R> ect = conjc(ldcx(eta, ot + r)), ect1 = conjc(ldcx(eta, ot + r1));
+        const Cx<R> gt = ldcx(g, ot + r), gt1 = ldcx(g, ot + r1);
+        const R h = (R)0.5;
+        if (a.kind == 21) {
+          // a = (ec_s(r+x) g_t + ec_t(r+x) g_s) e* / 2,  b = (g_s(r+x) ec_t + g_t(r+x) ec_s) e / 2
+          A = h * cmul(cmul(ecs1, gt) + cmul(ect1, gs), em);
+          B = h * cmul(cmul(gs1, ect) + cmul(gt1, ecs), ep);
+        } else {
+          // T2: a = (ec_s g_t(r+x) + ec_t g_s(r+x)) e / 2,  b = (g_s ec_t(r+x) + g_t ec_s(r+x)) e* / 2
+          A = h * cmul(cmul(ecs, gt1) + cmul(ect, gs1), ep);
+          B = h * cmul(cmul(gs, ect1) + cmul(gt, ecs1), em);
+        }
+      }
+      fa[q] = A;
+      fb[q] = B;
     }
-    reinterpret_cast<Cx<R>*>(fa)[q] = A;
-    reinterpret_cast<Cx<R>*>(fb)[q] = B;
     x += dx;
     y += dy;
     if (x >= L) {
@@ -164,7 +178,7 @@ int pair_fields_entry(int kind, const R* eta, const R* g, const R* ep, const int
   a.Nt = Ltau;
   a.fa = fa;
   a.fb = fb;
-  dim3 grid(npairs, Ltau);
+  dim3 grid((npairs + BB_GROUP - 1) / BB_GROUP, Ltau);
   k_bb_pair_fields<R><<<grid, 256, 0, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
