@@ -53,7 +53,7 @@ __device__ __forceinline__ Cx<R> conjc(Cx<R> a) {
 // site, and the first vector's values once per run of pairs that share it
 // (in torch.combinations order most consecutive pairs do), which halves the
 // L2 reads of T21 and T2.  Sites are walked without integer division.
-constexpr int BB_GROUP = 8;
+constexpr int BB_GROUP = 4;
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_bb_pair_fields(BondArgs a) {
