@@ -94,7 +94,20 @@ class BondBond:
         out[0, 0] += (g * ec).mean()
         return out
 
+    @staticmethod
+    def _reflect(a):
+        """a at -d: element (-dy mod Ly, -dx mod Lx) at (dy, dx)"""
+        return torch.roll(torch.flip(a, dims=(-2, -1)), shifts=(1, 1), dims=(-2, -1))
+
     def T2(self, eta, G_eta, boson):
+        """T2's two pair fields are T21's with a and b exchanged:
+        (ec_s g_t(r+x) + ec_t g_s(r+x)) e/2 is T21's b, and (g_s ec_t(r+x) +
+        g_t ec_s(r+x)) e*/2 is T21's a.  Its pair correlation is therefore T21's
+        at -d, and both add the same term at d = 0, so T2 is T21 reflected."""
+        return self._reflect(self.T21(eta, G_eta, boson))
+
+    def T2_direct(self, eta, G_eta, boson):
+        """T2 from its own pair fields (the reference's computation)."""
         ec, g, ph = self._fields(eta, G_eta, boson)
         out = -self._pair_mean("T2", eta, G_eta, boson)
         out[0, 0] += (g * ec).mean()
@@ -123,8 +136,8 @@ class BondBond:
 
     def get_bond_bond_per_b2(self, eta, G_eta, boson):
         """BB0_r, BB_r, B_r and BB_k (real parts; BB_k in ascending momentum order)."""
-        T = self.T1(eta, G_eta, boson) + self.T21(eta, G_eta, boson) + self.T2(eta, G_eta, boson) + \
-            self.T4(eta, G_eta, boson)
+        t21 = self.T21(eta, G_eta, boson)
+        T = self.T1(eta, G_eta, boson) + t21 + self._reflect(t21) + self.T4(eta, G_eta, boson)
         Tvv, Tv = self.Tvv(eta, G_eta, boson)
         BB_r = T * 2 + Tvv * 4
         BB_k = torch.fft.ifft2(BB_r, norm="forward")

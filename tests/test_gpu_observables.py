@@ -120,3 +120,19 @@ def test_pair_fields_and_kspace_sum_kernels(kind, cdt, tol):
     ops.bb_kspace_acc(A, B, S)  # accumulates
     want = 2 * (A.to(torch.complex128) * B.to(torch.complex128)).sum(dim=(0, 1)).reshape(-1)
     assert rel(S.cpu(), want.cpu()) < 1e-12
+
+
+@pytest.mark.parametrize("cdt,tol", [(torch.complex128, 1e-12), (torch.complex64, 1e-5)])
+def test_t2_is_t21_reflected(cdt, tol):
+    """T2 from T21 at -d (its pair fields are T21's exchanged) against T2 from its own pair
+    fields, on random noise vectors at L=8, Ltau=10."""
+    from qed_fermion_b200.observables import BondBond
+    L, Nt, nrv = 8, 10, 6
+    gen = torch.Generator(device="cpu").manual_seed(11)
+    mk = lambda *sh: torch.complex(torch.randn(*sh, generator=gen, dtype=torch.float64),
+                                    torch.randn(*sh, generator=gen, dtype=torch.float64)).to(cdt).to(DEV)
+    eta, g = mk(nrv, Nt * L * L), mk(nrv, Nt * L * L)
+    bos = (torch.rand(1, 2, L, L, Nt, generator=gen, dtype=torch.float64) * 6.2832).to(DEV)
+    bb = BondBond(L, Nt)
+    want = bb.T2_direct(eta, g, bos)
+    assert rel(bb.T2(eta, g, bos).cpu(), want.cpu()) < tol
