@@ -36,10 +36,10 @@ UNIT = "trajectories/hour"
 # DRAM bytes (read + write) per site and PCG iteration of k_pcg on this
 # workload, mixed precision, 2 right-hand sides: ncu --metrics
 # dram__bytes_read.sum,dram__bytes_write.sum of `bench.py --solve-only 482`
-# (profiles/k_pcg_mixed_L48_Lt480_rhs2.md)
 PCG_DRAM_BYTES_PER_SITE_ITER = 72.7
-# PCG iterations per solve of this workload (mixed, rtol 1e-10), as the GPU run
-# measures them; the CPU arms extrapolate a trajectory with it when they run alone
+# PCG iterations per solve of this workload (mixed, rtol 1e-10) as the GPU run
+# measures them: the CPU arms' fallback when they run neither a GPU solve nor
+# their own trajectory
 CG_ITERS_PER_SOLVE = 482
 
 
@@ -63,7 +63,12 @@ def parse_args(argv=None):
     ap.add_argument("--mhm-rhs", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--cg-iters-per-solve", type=float, default=None,
-                    help="reference arm: PCG iterations per solve used to extrapolate a trajectory")
+                    help="reference arm with --no-cpu-trajectory: PCG iterations per solve to extrapolate with")
+    ap.add_argument("--cpu-sample-iters", type=int, default=30,
+                    help="reference arm: PCG iterations in each timed sample step")
+    ap.add_argument("--no-cpu-trajectory", dest="cpu_trajectory", action="store_false",
+                    help="reference arm: skip the full CPU trajectory that sets the iteration count and checks "
+                         "the extrapolation")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--solve-only", type=int, default=0,
                     help="profiling mode: one PCG solve of the workload with exactly this many iterations")
@@ -143,54 +148,123 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # reference arm / CPU baseline: the oracle (CPU restatement of the reference)
 # ---------------------------------------------------------------------------
+class CpuPort:
+    """The CPU restatement of the path (the C/OpenMP port of the oracle,
+    oracle/qedf_cpu.c, complex128, all host threads) on one chain of the
+    bench workload: the same lattice, start and solver tolerance."""
+
+    def __init__(self, L, Ltau, seed):
+        import numpy as np
+        from oracle import cpu_port as C
+        from oracle import qedf_oracle as O
+        C.build()
+        self.C, self.O = C, O
+        self.L, self.Ltau = L, Ltau
+        rng = np.random.default_rng(seed)
+        Vs = L * L
+        self.boson = pi_flux_np(rng, L, Ltau, 1)
+        self.p0 = rng.standard_normal(self.boson.shape)
+        self.R = (rng.standard_normal(Ltau * Vs) + 1j * rng.standard_normal(Ltau * Vs)) / math.sqrt(2)
+        self.phi = O.ref_to_kernel_layout(self.boson)[0]
+        self.psi = O.mh_vec(self.phi[None], self.R.reshape(1, Ltau, Vs), L, 0.1)[0]
+        self.csr = C.csr_of(O.precon_tau_matrix(Ltau).real.astype(np.float64)) \
+            if Ltau >= O.precon_min_ltau() else None
+        self.cp = O.Couplings()
+        self.nth = C.threads()
+
+    def sample(self, n_it):
+        """One bounded sample: n_it PCG iterations, one fermion force and one
+        boson substep of the leapfrog.  Returns seconds per unit and in all."""
+        C, O = self.C, self.O
+        s = C.Pcg(self.phi, self.psi, self.L, 0.1, self.csr)
+        t0 = time.perf_counter()
+        for _ in range(n_it):
+            s.step()
+        t1 = time.perf_counter()
+        C.force(self.phi, s.x, self.L, 0.1)
+        t2 = time.perf_counter()
+        fb = O.force_b_plaq(self.boson, self.cp) + O.force_b_tau(self.boson, self.cp)
+        C.inner_boson_step(self.boson, self.p0, 0.05, fb, self.cp)
+        t3 = time.perf_counter()
+        return {"cg_iteration": (t1 - t0) / n_it, "force": t2 - t1, "boson_substep": t3 - t2,
+                "sample_s": t3 - t0}
+
+    def trajectory(self, n_leapfrog, delta_t, rtol):
+        """One full trajectory of this chain, timed: (seconds, iterations per solve, Delta H, seconds by part)."""
+        t0 = time.perf_counter()
+        H0, H1, iters, secs = self.C.trajectory(self.boson, self.p0, self.R, self.L, self.cp, delta_t, n_leapfrog,
+                                                rtol, 100000, self.csr)
+        return time.perf_counter() - t0, iters, H1 - H0, secs
+
+
+def cpu_traj_seconds(u, iters_per_solve, n_leapfrog, M=5):
+    """Seconds of one chain's trajectory from per-unit costs: n_leapfrog + 1
+    solves and forces, n_leapfrog * M boson substeps."""
+    return (n_leapfrog + 1) * (iters_per_solve * u["cg_iteration"] + u["force"]) + n_leapfrog * M * u["boson_substep"]
+
+
 def cpu_sample(L, Ltau, seed, seconds):
-    """Time the CPU restatement of the path on all host cores (the C/OpenMP port
-    of the oracle, oracle/qedf_cpu.c) on the same lattice and start: PCG
-    iterations (M^dag M, preconditioner, axpys, dots) and fermion forces.
-    Returns per-unit seconds, what was sampled and the thread count."""
-    import numpy as np
-    from oracle import cpu_port as C
-    from oracle import qedf_oracle as O
-    C.build()
-    rng = np.random.default_rng(seed)
-    Vs = L * L
-    phi = O.ref_to_kernel_layout(pi_flux_np(rng, L, Ltau, 1))[0]
-    v = (rng.standard_normal((Ltau, Vs)) + 1j * rng.standard_normal((Ltau, Vs))) / math.sqrt(2)
-    csr = C.csr_of(O.precon_tau_matrix(Ltau)) if Ltau >= O.precon_min_ltau() else None
-    t_it, t_force, n_it, n_f = C.time_sample(phi, v, L, 0.1, csr, seconds)
-    nth = C.threads()
-    return t_it, t_force, (f"{n_it} PCG iterations + {n_f} fermion forces of the C/OpenMP port of the oracle "
-                           f"(complex128) at L={L}, Ltau={Ltau} on {nth} threads"), nth
-
-
-def cpu_traj_per_hour(t_it, t_force, iters_per_solve, n_leapfrog):
-    solves = n_leapfrog + 1
-    t_traj = solves * (iters_per_solve * t_it + t_force)
-    return 3600.0 / t_traj
+    """Per-unit seconds of the CPU port on this workload, the medians of as
+    many bounded samples as fit in about ``seconds``.  Returns (units,
+    description, threads)."""
+    port = CpuPort(L, Ltau, seed)
+    port.sample(2)  # warm the caches and the thread pool
+    t0 = time.perf_counter()
+    runs = []
+    while not runs or time.perf_counter() - t0 < seconds:
+        runs.append(port.sample(24))
+    u = {k: statistics.median(r[k] for r in runs) for k in runs[0]}
+    return u, (f"{len(runs)} samples of 24 PCG iterations + 1 fermion force + 1 boson substep of the C/OpenMP port "
+               f"of the oracle (complex128) at L={L}, Ltau={Ltau} on {port.nth} threads"), port.nth
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's path on the
+    host cores.  Each step is a bounded sample (PCG iterations, a fermion
+    force, a boson substep of one chain); the value is the trajectories/hour
+    those per-unit costs imply with the iteration count of a full trajectory
+    that this arm runs and times first, whose measured time checks the
+    extrapolation."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    port = CpuPort(args.L, args.Ltau, args.seed)
+    port.sample(2)
+    check = None
     iters = args.cg_iters_per_solve
-    if iters is None:
-        iters = float(os.environ.get("QEDF_CG_ITERS_PER_SOLVE", CG_ITERS_PER_SOLVE))
-    per_step = []
-    sample, nth = "", 1
+    if args.cpu_trajectory:
+        t_traj, its, dH, secs = port.trajectory(args.n_leapfrog, args.delta_t, args.rtol)
+        iters = statistics.mean(its)
+        check = {"measured_s": t_traj, "iters_per_solve": iters, "delta_H": dH, "seconds_by_part": secs}
+    elif iters is None:
+        iters = CG_ITERS_PER_SOLVE
+    runs, step_s = [], []
     for k in range(args.warmup + args.steps):
-        t_it, t_force, sample, nth = cpu_sample(args.L, args.Ltau, args.seed + k, args.cpu_seconds / 2)
+        r = port.sample(args.cpu_sample_iters)
         if k >= args.warmup:
-            per_step.append(cpu_traj_per_hour(t_it, t_force, iters, args.n_leapfrog))
-    value = statistics.median(per_step)
+            runs.append(r)
+            step_s.append(r["sample_s"])
+    u = {k: statistics.median(r[k] for r in runs) for k in runs[0]}
+    t_extrap = cpu_traj_seconds(u, iters, args.n_leapfrog)
+    value = 3600.0 / t_extrap
+    sample = (f"each step: {args.cpu_sample_iters} PCG iterations + 1 fermion force + 1 boson substep of one chain, "
+              f"C/OpenMP port of the oracle (complex128) at L={args.L}, Ltau={args.Ltau} on {port.nth} threads; "
+              f"value extrapolated to a trajectory with {iters:.1f} PCG iterations per solve, "
+              f"{args.n_leapfrog + 1} solves and forces, {5 * args.n_leapfrog} boson substeps")
+    if check:
+        check["extrapolated_s"] = cpu_traj_seconds(u, check["iters_per_solve"], args.n_leapfrog)
+        check["extrapolation_error"] = check["extrapolated_s"] / check["measured_s"] - 1.0
+        sample += (f"; one full trajectory of this chain measured first: {check['measured_s']:.1f} s against "
+                   f"{check['extrapolated_s']:.1f} s extrapolated ({100 * check['extrapolation_error']:+.1f} %)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 3600e3 / value,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.mean(step_s),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128/f64 (C/OpenMP)",
         "data": "synthetic", "config": workload_config(args),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nth, "kind": "port",
-                         "sample": sample + f"; extrapolated with {iters:g} PCG iterations per solve, "
-                                            f"{args.n_leapfrog + 1} solves + forces per trajectory"},
+        "value_kind": "extrapolated from the timed samples (ms_per_step is one sample, not a trajectory)",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": port.nth, "kind": "port", "sample": sample,
+                         "s_per_unit": u},
+        "trajectory_check": check,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -468,12 +542,13 @@ def run_native(args):
     # --- CPU baseline (oracle restatement) on a bounded sample
     cpu = None
     if rank == 0 and world == 1 and args.cpu_seconds > 0 and not args.quick:
-        t_it, t_force, sample, nth = cpu_sample(L, Lt, seed, args.cpu_seconds)
+        u, sample, nth = cpu_sample(L, Lt, seed, args.cpu_seconds)
         ips = result.get("cg_iters_per_solve") or CG_ITERS_PER_SOLVE
-        cpu = {"value": cpu_traj_per_hour(t_it, t_force, ips, args.n_leapfrog), "unit": UNIT, "cores": nth,
-               "kind": "port", "sample": sample + f"; extrapolated with the {ips:.0f} PCG iterations per solve "
-                                                  f"this run needed, {args.n_leapfrog + 1} solves per trajectory",
-               "s_per_cg_iteration": t_it, "s_per_force": t_force}
+        cpu = {"value": 3600.0 / cpu_traj_seconds(u, ips, args.n_leapfrog), "unit": UNIT, "cores": nth,
+               "kind": "port", "sample": sample + f"; extrapolated to a trajectory with the {ips:.0f} PCG iterations "
+                                                  f"per solve this run needed, {args.n_leapfrog + 1} solves and "
+                                                  f"forces, {5 * args.n_leapfrog} boson substeps",
+               "s_per_unit": u}
 
     if rank == 0:
         line = {

@@ -240,7 +240,10 @@ int qedf_pcg_solve(const qedf_system* sys, int nsys, const void* boson, const vo
  * QEDF_ERR_SIZE.  Calls share the array: calls that overlap on the GPU race and
  * must be serialised by the caller.  The first call on a device looks up the
  * array's device address (once per device, that device current); make it
- * before any stream capture begins.  It calls no cudaMalloc or other allocator.
+ * before any stream capture begins.  That address is kept for the life of the
+ * process: a process that resets the device (cudaDeviceReset) or otherwise
+ * tears down its primary context must not call this entry point afterwards.
+ * It calls no cudaMalloc or other allocator.
  * ------------------------------------------------------------------------- */
 #define QEDF_PCG_STATIC_SCRATCH_BYTES (64ll << 20)
 

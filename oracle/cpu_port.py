@@ -129,3 +129,73 @@ def time_sample(phi, b, L, dtau, csr, seconds):
         force(phi, b, L, dtau)
         n_f += 1
     return t_it, (time.perf_counter() - t1) / n_f, n_it, n_f
+
+
+def solve(phi, b, L, dtau, csr, rtol, max_iter):
+    """PCG on M^dag M x = b until the iterated relative residual is at most
+    ``rtol``: the C port's iteration, the stopping test of ``pcg_single``.
+    Returns (x, iterations, relative residual)."""
+    s = Pcg(phi, b, L, dtau, csr)
+    bb = float(np.vdot(b, b).real)
+    it = 0
+    while it < max_iter and s.rr > rtol * rtol * bb:
+        s.step()
+        it += 1
+    return s.x, it, (s.rr / bb) ** 0.5
+
+
+def inner_boson_step(x, p, dt, fb, cp, M=5):
+    """One of the M boson-only substeps of ``leapfrog_cmp``
+    (``hmc_sampler_batch.py:2332-2347``), numpy, reference layout."""
+    from . import qedf_oracle as O
+    p = p + fb * dt / 2 / M
+    x = x + p / cp.m * dt / M
+    fb = O.force_b_plaq(x, cp) + O.force_b_tau(x, cp)
+    p = p + fb * dt / 2 / M
+    return x, p, fb
+
+
+def trajectory(boson_ref, p0, R, L, cp, delta_t, n_leapfrog, rtol, max_iter, csr, M=5):
+    """One HMC trajectory of one chain (``leapfrog_proposer5``,
+    ``hmc_sampler_batch.py:2366-2625``, as ``qedf_oracle.trajectory``): the
+    fermion solves and forces on the C port, the boson parts in numpy.
+    ``boson_ref`` / ``p0``: ``[1, 2, L, L, Nt]``; ``R``: ``[Nt*Vs]``.
+    Returns (H0, H_fin, PCG iterations per solve, seconds by part)."""
+    from . import qedf_oracle as O
+    Nt = boson_ref.shape[-1]
+    Vs = L * L
+    secs = {"solve": 0.0, "force": 0.0, "boson": 0.0}
+
+    def fermion(x):
+        phi = O.ref_to_kernel_layout(x)[0]
+        t0 = time.perf_counter()
+        xi, it, _ = solve(phi, psi, L, cp.dtau, csr, rtol, max_iter)
+        t1 = time.perf_counter()
+        F = force(phi, xi, L, cp.dtau)
+        secs["solve"] += t1 - t0
+        secs["force"] += time.perf_counter() - t1
+        return O.kernel_to_ref_layout(F[None], L), xi, it
+
+    def H(x, p, xi):
+        return float(O.action_boson_tau(x, cp)[0] + O.action_boson_plaq(x, cp)[0] + (p ** 2).sum() / (2 * cp.m)
+                     + np.vdot(psi, xi).real)
+
+    x = boson_ref.copy()
+    p = p0.copy()
+    psi = O.mh_vec(O.ref_to_kernel_layout(x), R.reshape(1, Nt, Vs), L, cp.dtau, cp.t)[0]
+    Ff, xi, it = fermion(x)
+    iters = [it]
+    H0 = H(x, p, xi)
+    t0 = time.perf_counter()
+    fb = O.force_b_plaq(x, cp) + O.force_b_tau(x, cp)
+    secs["boson"] += time.perf_counter() - t0
+    for _ in range(n_leapfrog):
+        p = p + delta_t / 2 * Ff
+        t0 = time.perf_counter()
+        for _ in range(M):
+            x, p, fb = inner_boson_step(x, p, delta_t, fb, cp, M)
+        secs["boson"] += time.perf_counter() - t0
+        Ff, xi, it = fermion(x)
+        iters.append(it)
+        p = p + delta_t / 2 * Ff
+    return H0, H(x, p, xi), iters, secs

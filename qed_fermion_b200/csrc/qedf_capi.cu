@@ -181,27 +181,9 @@ int pcg_solve_ws(const qedf_system* sys, int nsys, const void* boson, const void
   if (!aligned16(boson) || !aligned16(b) || !aligned16(x) || !aligned16(workspace)) return QEDF_ERR_ARG;
   if (opts->max_iter < 0 || !(opts->rtol >= 0)) return QEDF_ERR_ARG;
   const int sb = opts->mode == QEDF_PCG_PLAIN_F64 ? 8 : 4;
-  const size_t need = pcg_workspace_bytes(p, sb);
-  if (ws_bytes < (int64_t)need) return QEDF_ERR_ARG;
-  // carve the workspace
-  unsigned char* w = reinterpret_cast<unsigned char*>(workspace);
-  const size_t vecb = ((size_t)p.nvec_total * 2 * sb + 255) / 256 * 256;
-  p.r = w;
-  p.p0 = w + vecb;
-  p.p1 = w + 2 * vecb;
-  p.z = w + 3 * vecb;
-  p.Op = w + 4 * vecb;
-  size_t off = 5 * vecb;
-  if (p.mode == QEDF_PCG_MIXED) {
-    p.xlo = w + off;
-    off += vecb;
-  }
-  p.acc = reinterpret_cast<double*>(w + off);
-  const size_t accb = ((sizeof(double) * 9 * p.nrhs) + 255) / 256 * 256;
-  off += accb;
-  p.bar = reinterpret_cast<unsigned int*>(w + off);
-  off += 256;
-  p.ptab = reinterpret_cast<float*>(w + off);
+  if (ws_bytes < (int64_t)pcg_workspace_bytes(p, sb)) return QEDF_ERR_ARG;
+  size_t zero_bytes = 0;
+  pcg_carve(p, sb, workspace, &zero_bytes);
   p.phi = boson;
   p.b = b;
   p.x = x;
@@ -217,7 +199,7 @@ int pcg_solve_ws(const qedf_system* sys, int nsys, const void* boson, const void
   p.timeout_cycles = (long long)(tmo * (double)clk_khz);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   // accumulators and barrier state start at zero; preconditioner tables
-  if (int e2 = launch_pcg_prep(p, (int)((accb + 256) / 4), st)) return e2;
+  if (int e2 = launch_pcg_prep(p, (int)(zero_bytes / 4), st)) return e2;
   return launch_pcg(p, opts->by, st);
 }
 

@@ -137,6 +137,7 @@ struct PcgParams {
 };
 
 size_t pcg_workspace_bytes(const PcgParams& p, int sloppy_bytes);
+size_t pcg_carve(PcgParams& p, int sloppy_bytes, void* workspace, size_t* zero_bytes);
 int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts* o);
 int launch_pcg(PcgParams& p, int by, cudaStream_t st);
 int launch_pcg_prep(const PcgParams& p, int zero_words, cudaStream_t st);

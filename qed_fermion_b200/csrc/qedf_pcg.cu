@@ -925,12 +925,39 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
   return QEDF_OK;
 }
 
-size_t pcg_workspace_bytes(const PcgParams& p, int sloppy_bytes) {
+// The workspace layout, in one place: r, p0, p1, z, Op (and x_lo in mixed
+// mode) in the sloppy precision, the double accumulators (ACC_PER_RHS per
+// right-hand side), 256 bytes of grid-barrier words and the preconditioner
+// tables, each 256-byte aligned.  Returns the bytes the layout needs; with a
+// workspace it also points p's buffers into it, and *zero_bytes receives the
+// length of the block that starts at zero every solve (accumulators and
+// barrier words, contiguous from p.acc).
+size_t pcg_carve(PcgParams& p, int sloppy_bytes, void* workspace, size_t* zero_bytes) {
   const size_t vecb = align_up((size_t)p.nvec_total * 2 * sloppy_bytes, 256);
-  const int nv = p.mode == QEDF_PCG_MIXED ? 6 : 5;
+  const bool mixed = p.mode == QEDF_PCG_MIXED;
+  const int nv = mixed ? 6 : 5;
   const size_t accb = align_up(sizeof(double) * ACC_PER_RHS * p.nrhs, 256);
+  const size_t barb = 256;
   const size_t tabb = align_up(sizeof(float) * (size_t)p.ptab_len, 256);
-  return nv * vecb + accb + 256 + tabb;
+  if (zero_bytes) *zero_bytes = accb + barb;
+  if (workspace) {
+    unsigned char* w = static_cast<unsigned char*>(workspace);
+    p.r = w;
+    p.p0 = w + vecb;
+    p.p1 = w + 2 * vecb;
+    p.z = w + 3 * vecb;
+    p.Op = w + 4 * vecb;
+    p.xlo = mixed ? w + 5 * vecb : nullptr;
+    p.acc = reinterpret_cast<double*>(w + nv * vecb);
+    p.bar = reinterpret_cast<unsigned int*>(w + nv * vecb + accb);
+    p.ptab = reinterpret_cast<float*>(w + nv * vecb + accb + barb);
+  }
+  return nv * vecb + accb + barb + tabb;
+}
+
+size_t pcg_workspace_bytes(const PcgParams& p, int sloppy_bytes) {
+  PcgParams q = p;
+  return pcg_carve(q, sloppy_bytes, nullptr, nullptr);
 }
 
 // Per solve: zero the accumulators and barrier words, and write each system's

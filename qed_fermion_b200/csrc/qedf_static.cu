@@ -22,7 +22,10 @@
 // In host code the name g_pcg_scratch is only a host-side stand-in, not a
 // device address.  The device address is looked up with cudaGetSymbolAddress
 // once per device, with that device current, by the first call on it; make
-// that first call before any stream capture begins.
+// that first call before any stream capture begins.  The address is cached for
+// the life of the process, so it is stale after cudaDeviceReset (the module is
+// loaded again in the new context, possibly elsewhere): a process that resets
+// a device must not call this entry point afterwards.
 #include <cstdint>
 #include <mutex>
 

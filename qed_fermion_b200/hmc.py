@@ -141,12 +141,17 @@ class HmcSampler:
         (a dict with 'boson' and optionally 'delta_t_tensor', or a bare tensor)."""
         loaded = torch.load(path, map_location="cpu")
         boson = loaded["boson"] if isinstance(loaded, dict) else loaded
-        if tuple(boson.shape[1:]) != (2, self.Lx, self.Ly, self.Ltau):
-            raise RuntimeError(f"checkpoint field has shape {tuple(boson.shape)}, expected [bs, 2, {self.Lx}, "
-                               f"{self.Ly}, {self.Ltau}]")
-        self.boson = boson.to(device=self.device, dtype=self.dtype)
+        if tuple(boson.shape) != (self.bs, 2, self.Lx, self.Ly, self.Ltau):
+            raise RuntimeError(f"checkpoint field has shape {tuple(boson.shape)}, expected [{self.bs}, 2, "
+                               f"{self.Lx}, {self.Ly}, {self.Ltau}] (the sampler's chains)")
+        dt = None
         if isinstance(loaded, dict) and "delta_t_tensor" in loaded:
-            self.delta_t_tensor = loaded["delta_t_tensor"].to(device=self.device, dtype=torch.float64)
+            dt = loaded["delta_t_tensor"].reshape(-1)
+            if dt.numel() != self.bs:
+                raise RuntimeError(f"checkpoint has {dt.numel()} step sizes for {self.bs} chains")
+        self.boson = boson.to(device=self.device, dtype=self.dtype)
+        if dt is not None:
+            self.delta_t_tensor = dt.to(device=self.device, dtype=torch.float64)
         return self.boson
 
     def initialize_boson_ensemble(self, data_folder, specifics, steps=range(4000, 10001, 500)):

@@ -1,10 +1,10 @@
 """Generate golden vectors by running the reference's own CPU path in complex128.
 
-Run in a container where the reference source tree is present:
+Run where the reference source tree is present, giving its root directory:
 
-    python tests/golden/make_golden.py /root/reference          # golden_ref.npz, golden_traj.npz
-    python tests/golden/make_golden.py /root/reference bond     # golden_bond.npz
-    python tests/golden/make_golden.py /root/reference fourier  # golden_fourier_mass.npz
+    python tests/golden/make_golden.py <reference-root>          # golden_ref.npz, golden_traj.npz
+    python tests/golden/make_golden.py <reference-root> bond     # golden_bond.npz
+    python tests/golden/make_golden.py <reference-root> fourier  # golden_fourier_mass.npz
 
 The reference module ``qed_fermion.hmc_sampler_batch`` imports ``matplotlib``
 and ``matlab.engine`` at module level; neither is needed for the CPU path, so
@@ -255,7 +255,7 @@ def gen_estimator(H, out, rng):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1]
     H, PM = import_reference(ref_root)
     rng = np.random.default_rng(20240611)
     out = {}
@@ -361,6 +361,8 @@ def main_fourier(ref_root):
 
 
 if __name__ == "__main__":
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py <reference-root> [bond|fourier]")
     if len(sys.argv) > 2 and sys.argv[2] == "bond":
         main_bond(sys.argv[1])
     elif len(sys.argv) > 2 and sys.argv[2] == "fourier":

@@ -58,3 +58,18 @@ def test_initialize_from_ensemble(tmp_path):
     e.initialize_boson_ensemble(str(tmp_path / "empty"), "spec")
     ref = _sampler(seed=11)
     assert torch.equal(e.boson, ref.initialize_boson_pi_flux_randn_matfree())
+
+
+def test_rejects_other_chain_counts(tmp_path):
+    """A field saved with another number of chains, or step sizes that do not
+    match its chains, is refused rather than broadcast."""
+    torch.save({"boson": torch.randn(3, 2, 4, 4, 10), "delta_t_tensor": torch.full((3,), 0.03)},
+               tmp_path / "three.pt")
+    torch.save({"boson": torch.randn(2, 2, 4, 4, 10), "delta_t_tensor": torch.full((3,), 0.03)},
+               tmp_path / "bad_dt.pt")
+    h = _sampler()
+    with pytest.raises(RuntimeError, match="chains"):
+        h.load_boson_checkpoint(str(tmp_path / "three.pt"))
+    with pytest.raises(RuntimeError, match="step sizes"):
+        h.load_boson_checkpoint(str(tmp_path / "bad_dt.pt"))
+    assert h.boson is None
