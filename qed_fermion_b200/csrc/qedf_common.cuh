@@ -144,6 +144,97 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Bulk copies global -> shared by the copy engine (cp.async.bulk, no tensor
+// map, no multicast), completed on an mbarrier through its transaction count.
+// Source and destination are 16-byte aligned and the size is a multiple of 16.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+// one arrival that also announces `bytes` of copies to come
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// orders this thread's view of global memory (generic proxy, e.g. data other
+// blocks wrote before a grid barrier) before its following bulk copies
+__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;\n" ::: "memory"); }
+__device__ __forceinline__ bool mbar_test_parity(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// wait for phase `parity` of the mbarrier to complete; false when `budget` SM
+// cycles passed first (the wait is always bounded)
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, long long budget) {
+  if (mbar_test_parity(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_test_parity(bar, parity))
+    if (clock64() - t0 > budget) return false;
+  return true;
+}
+
+// Two shared-memory buffers of NARR whole slices each, filled by bulk copies
+// that one thread issues; stage j of a sequence goes to buffer j % 2.  The
+// caller guarantees that every thread finished reading stage j - 2 (a block
+// barrier lies between) before stage j is issued.  `uses` counts the
+// completed phases of each buffer's mbarrier, identically in every thread.
+template <int NARR>
+struct SliceStages {
+  unsigned long long* bar;  // [2], static shared memory, initialised once per kernel
+  unsigned char* buf;       // [2][NARR][bytes]
+  unsigned bytes;           // bytes of one slice array
+  unsigned uses[2];
+
+  __device__ void setup(unsigned long long* bars, unsigned char* buffers, unsigned slice_bytes) {
+    bar = bars;
+    buf = buffers;
+    bytes = slice_bytes;
+    uses[0] = uses[1] = 0;
+  }
+  // once per kernel, by every thread (contains a block barrier)
+  __device__ static void init_barriers(unsigned long long* bars) {
+    if (threadIdx.x == 0) {
+      mbar_init(bars, 1);
+      mbar_init(bars + 1, 1);
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
+  __device__ __forceinline__ unsigned char* slot(int j, int k) const {
+    return buf + ((size_t)(j & 1) * NARR + k) * bytes;
+  }
+  // thread 0 only: copy the arrays src[k] with bit k of `mask` into stage j
+  __device__ void issue(int j, const void* const (&src)[NARR], unsigned mask) {
+    unsigned n = 0;
+#pragma unroll
+    for (int k = 0; k < NARR; ++k) n += (mask >> k) & 1u;
+    fence_proxy_async_global();
+    mbar_arrive_expect_tx(bar + (j & 1), n * bytes);
+#pragma unroll
+    for (int k = 0; k < NARR; ++k)
+      if ((mask >> k) & 1u) bulk_copy_g2s(slot(j, k), src[k], bytes, bar + (j & 1));
+  }
+  // every thread: wait for stage j; false if the bounded wait gave up
+  __device__ bool wait(int j, long long budget) {
+    const int b = j & 1;
+    const bool ok = mbar_wait_bounded(bar + b, uses[b] & 1u, budget);
+    ++uses[b];
+    return ok;
+  }
+};
+
 // Coefficients of the checkerboard factors F_g = c_g (I + t_g K_g):
 // g1 uses cosh/tanh(dtau), g2..g4 cosh/tanh(dtau/2); Cb = c1 c2^2 c3^2 c4^2
 // is the scalar that B = F4 F3 F2 F1 F2 F3 F4 carries in front of the

@@ -18,6 +18,8 @@ struct OpArgs {
   int rhs_per_phi;  // consecutive vectors sharing one angle array
   int T;            // slab length (0 = auto)
   int xs;           // allow the warp-shuffle engine (single precision, L <= 64)
+  int stage;        // allow the staged M^dag M engine (single precision)
+  int stage_off;    // bytes: start of the slice stages in dynamic shared memory
   double c1, ch, t1, th, Cb;
 };
 
@@ -64,6 +66,8 @@ struct KickArgs {
 };
 
 int num_sms();
+// count of operator-kernel waits that gave up since the last read (then cleared)
+int read_wait_timeouts(unsigned int* count);
 // tile height (rows of the 2 x by site block per thread) for an L x L slice;
 // requested = 0 picks automatically; -1 if no valid tile exists
 int pick_by(int L, int requested, int real_bytes);
@@ -109,6 +113,8 @@ struct PcgParams {
   PcgSys sys[PCG_MAX_SYS];
   int mode;  // QEDF_PCG_PLAIN_F32, QEDF_PCG_PLAIN_F64, QEDF_PCG_MIXED
   int xs;    // allow the warp-shuffle engine for the single-precision iterations
+  int stage; // 1: allow the staged operator engine (EC_STAGE) where its shared memory fits
+  int stage_off;  // bytes: start of the operator passes' slice stages in dynamic shared memory
   int l2;    // 0: L2 persisting window over the iteration vectors when they fit; -1: off
   int max_iter, ru_interval;
   double rtol, ru_delta;

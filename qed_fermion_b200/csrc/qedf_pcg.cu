@@ -216,8 +216,11 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   constexpr bool PHS_S = (ECS & EC_PHS) != 0, STASH_S = (ECS & EC_NOSTASH) == 0;
   constexpr bool XS_S = (ECS & EC_XS) != 0;
   constexpr bool PHS_H = (ECH & EC_PHS) != 0, STASH_H = (ECH & EC_NOSTASH) == 0;
-  extern __shared__ __align__(16) unsigned char dsm[];
+  constexpr bool STG_S = (ECS & EC_STAGE) != 0;
+  static_assert(!STG_S || (STASH_S && !XS_S), "the staged engine keeps y_t in the stash");
+  extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ RhsState st;
+  __shared__ unsigned long long stg_bar[2];
   constexpr bool MIXED = !std::is_same<RS, RH>::value;
   // lattice side: compiled in (every system has it) or per system
   constexpr int LT = ec_fixed_l(ECS);
@@ -238,6 +241,14 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   constexpr int CHC = PCG_CHUNK;
   constexpr int PPR = CHC / 2;    // site pairs per row of a unit
 
+  // slice stages of the operator passes (EC_STAGE): two buffers of z, p_old
+  // and x_lo slices behind the slice engine's tables
+  SliceStages<3> stg;
+  const long long budget_stage = p.timeout_cycles;
+  if constexpr (STG_S) {
+    SliceStages<3>::init_barriers(stg_bar);
+    stg.setup(stg_bar, dsm + p.stage_off, 0);
+  }
   for (int v = tid; v < NV; v += blockDim.x) {
     st.active[v] = 1;
     st.iters[v] = 0;
@@ -522,6 +533,131 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     __syncthreads();
   };
 
+  // The same pass with the slices of z, p_old and x_lo staged whole in shared
+  // memory (EC_STAGE): stage j holds slice tp + j of the sequence tp, a, ...,
+  // bnd (bulk copies issued by thread 0 one slice ahead), so the slice loop
+  // reads its inputs from shared memory and never waits on a global load.
+  auto operator_unit_staged = [&](int u, int slot) {
+    if constexpr (STG_S) {
+    const int s = find_sys_A(p, u);
+    const PcgSys& S = p.sys[s];
+    const int lu = u - S.unitA0;
+    const int v = S.rhs0 + lu / S.nslab;
+    const int a = (lu % S.nslab) * S.T;
+    const int bnd = min(a + S.T, S.Nt);
+    const int Nt = S.Nt, Vs = SL(S) * SL(S);
+    const size_t sv = 2 * (size_t)Vs;
+    Slice<RS, BY, PHS_S, XS_S, LT> E;
+    E.init(SL(S), dsm, 2, (RS)p.c1, (RS)p.ch, tid);
+    const int64_t vb = 2 * vec_base(s, v);
+    const A* phi = phi_all + S.phi0 + (S.shared ? 0 : (int64_t)(v - S.rhs0) * Nt * sv);
+    const RS beta = (RS)st.beta[v];
+    const bool has_old = st.iters[v] > 0;
+    const bool pend = st.pending[v];
+    const RS al_old = (RS)st.alpha[v];
+    RS* xl = xs + vb;
+    const RS* pold = reinterpret_cast<const RS*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
+    RS* pnew = reinterpret_cast<RS*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
+    const RS* zz = (S.precon ? zbuf : reinterpret_cast<const RS*>(r)) + vb;
+    RS* O = Op + vb;
+    const RS t1 = (RS)p.t1, th = (RS)p.th, Cb = (RS)p.Cb;
+    stg.bytes = (unsigned)(Vs * sizeof(Cx<RS>));
+    const int nT = bnd - a;  // own slices
+    const int tp = (a - 1 + Nt) % Nt;
+    auto slice_of = [&](int j) { const int t = tp + j; return t >= Nt ? t - Nt : t; };
+    auto issue = [&](int j) {
+      if (tid != 0 || j > nT + 1) return;
+      const int t = slice_of(j);
+      const void* src[3] = {zz + t * sv, pold + t * sv, xl + t * sv};
+      const bool own = j >= 1 && j <= nT;
+      stg.issue(j, src, 1u | (has_old ? 2u : 0u) | ((own && pend && has_old) ? 4u : 0u));
+    };
+    auto wait = [&](int j) {
+      if (!stg.wait(j, budget_stage)) atomicExch(p.bar + 2, (unsigned int)QEDF_ERR_TIMEOUT);
+    };
+    // p = z + beta p_old of stage j; on own slices also x_lo += alpha_old p_old
+    auto getp = [&](Cx<RS> (&X)[BY][2], int j, bool own) {
+      if (!E.on) return;
+      E.load_coherent(X, reinterpret_cast<const RS*>(stg.slot(j, 0)));
+      if (has_old) {
+        Cx<RS> T0[BY][2];
+        E.load_coherent(T0, reinterpret_cast<const RS*>(stg.slot(j, 1)));
+        if (own && pend) {
+          Cx<RS> XL[BY][2];
+          E.load_coherent(XL, reinterpret_cast<const RS*>(stg.slot(j, 2)));
+#pragma unroll
+          for (int q = 0; q < BY; ++q)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              XL[q][c].re = fma(al_old, T0[q][c].re, XL[q][c].re);
+              XL[q][c].im = fma(al_old, T0[q][c].im, XL[q][c].im);
+            }
+          E.store(xl + slice_of(j) * sv, XL);
+        }
+#pragma unroll
+        for (int q = 0; q < BY; ++q)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            X[q][c].re = fma(beta, T0[q][c].re, X[q][c].re);
+            X[q][c].im = fma(beta, T0[q][c].im, X[q][c].im);
+          }
+      }
+    };
+    Cx<RS> X0[BY][2], X1[BY][2], Y[BY][2];
+    double pap = 0;
+    issue(0);
+    issue(1);
+    wait(0);
+    getp(X0, 0, false);
+    wait(1);
+    getp(X1, 1, true);
+    if (E.on) E.store(pnew + a * sv, X1);
+    A ang[BY][4];
+    if constexpr (!PHS_S) E.load_angles(ang, phi + a * sv);
+    E.phases(phi + tp * sv, t1, th);  // block barrier: stage 0 is read
+    issue(2);
+    E.template applyB<FAC_TILDE>(X0);
+    axpy_blk<RS, BY>(Y, X1, sigma_of<RS>(tp, Nt) * Cb, X0);  // y_a
+    E.park(Y);
+    copy_blk<RS, BY>(X0, X1);
+    for (int i = 0; i < nT; ++i) {
+      const int t = a + i, tn = (t + 1) % Nt;
+      issue(i + 3);  // into the buffer of stage i + 1, read before the last barriers
+      wait(i + 2);
+      getp(X1, i + 2, t + 1 < bnd);
+      if (E.on && t + 1 < bnd) E.store(pnew + tn * sv, X1);
+      if constexpr (!PHS_S) {
+        E.phases_from(ang, t1, th);
+        if (t + 1 < bnd) E.load_angles(ang, phi + (t + 1) * sv);
+      } else {
+        E.phases(phi + t * sv, t1, th);
+      }
+      const RS sg = sigma_of<RS>(t, Nt) * Cb;
+      E.template applyB<FAC_TILDE>(X0);       // B_t p_t
+      axpy_blk<RS, BY>(Y, X1, sg, X0);         // y_{t+1}
+      E.unpark(X0);                            // y_t
+      E.park(Y);
+      if (E.on) {
+        RS sq = 0;
+#pragma unroll
+        for (int q = 0; q < BY; ++q)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) sq = fma(X0[q][c].re, X0[q][c].re, fma(X0[q][c].im, X0[q][c].im, sq));
+        pap += (double)sq;
+      }
+      E.template applyB<FAC_TILDE, 1>(Y);     // B_t y_{t+1}
+      if (E.on) {
+        axpy_blk<RS, BY>(Y, X0, sg, Y);        // (M^dag M p)_t
+        E.store(O + t * sv, Y);
+      }
+      copy_blk<RS, BY>(X0, X1);
+    }
+    const double sum = block_sum_d(pap, st.red);
+    if (tid == 0) atomicAdd(acc.pAp + slot * NV + v, sum);
+    __syncthreads();
+    }
+  };
+
   // r = b - M^dag M x in the high precision (mixed mode), rr_true
   auto operator_unit_true_residual = [&](int u) {
     const int s = find_sys_A(p, u);
@@ -754,7 +890,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     for (int u = blockIdx.x; u < p.unitsA; u += gridDim.x) {
       const int s = find_sys_A(p, u);
       const int v = p.sys[s].rhs0 + (u - p.sys[s].unitA0) / p.sys[s].nslab;
-      if (st.active[v]) operator_unit_sloppy(u, aslot);
+      if (st.active[v]) {
+        if constexpr (STG_S) operator_unit_staged(u, aslot);
+        else operator_unit_sloppy(u, aslot);
+      }
     }
     // the rr/rz slot that BC will fill was last read before the previous barrier
     if (blockIdx.x == 0)
@@ -823,6 +962,9 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
 // host side
 // ---------------------------------------------------------------------------
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+// shared memory of the operator passes' slice stages: 2 buffers x 3 slices
+template <typename RS>
+static size_t pcg_stage_bytes(int L) { return 2 * 3 * (size_t)L * L * sizeof(Cx<RS>); }
 
 // Slab length of the operator units: units are dealt to the blocks in turn,
 // so the busiest block runs ceil(units / nblk) units of T slices plus one
@@ -853,6 +995,7 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
   p.mode = o->mode;
   p.nsys = nsys;
   p.xs = 1;
+  p.stage = o->stage < 0 ? 0 : 1;
   p.l2 = o->l2_persist < 0 ? -1 : 0;
   if (o->chunk != 0 && o->chunk != PCG_CHUNK) return QEDF_ERR_ARG;
   p.CH = PCG_CHUNK;
@@ -1056,6 +1199,10 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   if (eng_threads > MaxT<BY, ECS>::value) return QEDF_ERR_SIZE;
   const int threads = std::min(MaxT<BY, ECS>::value, std::max(128, eng_threads));
   size_t smem = slice_smem_bytes<RS, ECS>(Lmax, BY, 2);
+  if (ECS & EC_STAGE) {
+    p.stage_off = (int)align_up(smem, 128);
+    smem = p.stage_off + pcg_stage_bytes<RS>(Lmax);
+  }
   smem = std::max(smem, slice_smem_bytes<RH, ECH>(Lmax, BY, 2));
   // elementwise units: the r column, and in single precision the staging
   // area of the update pass
@@ -1111,6 +1258,12 @@ int launch_pcg_prep(const PcgParams& p, int zero_words, cudaStream_t st) {
 }
 
 static bool fits(size_t engine_bytes) { return engine_bytes + sizeof(RhsState) <= 227 * 1024; }
+// the staged engine: its tables plus two stages of three slices
+template <typename RS, int ECS>
+static bool fits_staged(int L, int BY) {
+  return align_up(slice_smem_bytes<RS, ECS>(L, BY, 2), 128) + pcg_stage_bytes<RS>(L) + sizeof(RhsState) <=
+         227 * 1024;
+}
 
 // Engines compiled for a fixed lattice side (with_fixed_l) when every system
 // has that side; otherwise the run-time-L engine.
@@ -1135,6 +1288,8 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
   const bool xs = p.xs && pow2 && xs_possible(Lmax) && slice_threads(Lmax, BY, true) <= MaxT<BY, EC_XS>::value;
   switch (p.mode) {
     case QEDF_PCG_PLAIN_F32:
+      if (p.stage && fits_staged<float, 0>(Lmax, BY))
+        return launch_pcg_fl<float, float, float, BY, EC_STAGE, EC_STAGE>(p, st);
       if (xs && fits(slice_smem_bytes<float, 0>(Lmax, BY, 2)))
         return launch_pcg_t<float, float, float, BY, EC_XS, EC_XS>(p, st);
       if (fits(slice_smem_bytes<float, 0>(Lmax, BY, 2)))
@@ -1147,6 +1302,8 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
         return launch_pcg_fl<double, double, double, BY, 0, 0>(p, st);
       return launch_pcg_t<double, double, double, BY, EC_NOSTASH, EC_NOSTASH>(p, st);
     case QEDF_PCG_MIXED:
+      if (p.stage && fits_staged<float, 0>(Lmax, BY) && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
+        return launch_pcg_fl<float, double, float, BY, EC_STAGE, EC_PHS>(p, st);
       if (xs && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
         return launch_pcg_t<float, double, float, BY, EC_XS, EC_PHS>(p, st);
       if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))

@@ -50,9 +50,12 @@ struct MaxThreads {
 //   EC_XS      exchanges of the x-bond factors by warp shuffles: a warp holds
 //              whole rows of tiles (L/2 <= 32 tiles per row, padded to a power
 //              of two), so only the y-bond factors need a block barrier
+//   EC_STAGE   the vector slices an operator pass reads are staged whole in
+//              shared memory by bulk copies one slice ahead (SliceStages), so
+//              no thread waits on a global load in the slice loop
 //   EC_L(l)    (bits 8 and up) the lattice side fixed at compile time, so the
 //              engine's index arithmetic folds into constants; 0 = run-time L
-enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4 };
+enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_STAGE = 8 };
 __host__ __device__ constexpr int EC_L(int l) { return l << 8; }
 __host__ __device__ constexpr int ec_fixed_l(int ec) { return ec >> 8; }
 // Lattice sides with engines compiled for their size: the benchmark

@@ -1,0 +1,77 @@
+"""The staged operator engine (input slices copied whole into shared memory by
+bulk copies, one slice ahead) against the engine that loads them directly:
+the same arithmetic on the same values, so the PCG results agree bit for bit,
+and the staged M^dag M against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import qedf_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda:0") if torch.cuda.is_available() else None
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("needs a CUDA device")
+    from qed_fermion_b200 import build
+    build.build()
+    torch.cuda.set_device(DEV)
+
+
+def _case(L, Nt, nrhs, seed):
+    rng = np.random.default_rng(seed)
+    x = np.arange(L)[:, None]
+    y = np.arange(L)[None, :]
+    sg = 1 - 2 * ((x + y) % 2)
+    boson = np.zeros((nrhs, 2, L, L, Nt))
+    boson[:, 0] = (sg * np.pi / 4)[None, :, :, None]
+    boson[:, 1] = (-sg * np.pi / 4)[None, :, :, None]
+    boson += 0.1 * rng.standard_normal(boson.shape)
+    b = (rng.standard_normal((nrhs, Nt * L * L)) + 1j * rng.standard_normal((nrhs, Nt * L * L))) / np.sqrt(2)
+    return O.ref_to_kernel_layout(boson).reshape(-1), b.reshape(-1)
+
+
+@pytest.mark.parametrize("mode", ["mixed", "fp32"])
+@pytest.mark.parametrize("systems", [
+    [(48, 24, 2)],               # the engine compiled for L = 48
+    [(12, 40, 2)],               # run-time L, preconditioned
+    [(20, 14, 3)],               # no preconditioner (Ltau < 26)
+    [(12, 30, 1), (18, 36, 2)],  # two lattices in one launch
+])
+def test_pcg_staged_engine_is_bit_identical(mode, systems):
+    from qed_fermion_b200 import _lib
+    from qed_fermion_b200.solver import PcgSolver, System
+    sysl = [System(L, Nt, k) for L, Nt, k in systems]
+    phis, bs = zip(*[_case(L, Nt, k, seed=L + Nt + k) for L, Nt, k in systems])
+    out = []
+    for stage in (True, False):
+        s = PcgSolver(sysl, mode=mode, rtol=1e-14, max_iter=60, device=DEV, stage=stage, timeout_ms=500.0)
+        res = s.solve(torch.tensor(np.concatenate(phis), dtype=s.angle_dtype, device=DEV),
+                      torch.tensor(np.concatenate(bs), dtype=s.vec_dtype, device=DEV))
+        torch.cuda.synchronize()
+        out.append((res.x.clone(), res.iters.clone(), res.relres.clone(), res.status.clone()))
+    assert out[0][3].cpu().tolist() == out[1][3].cpu().tolist()
+    assert set(out[0][3].cpu().tolist()) <= {0, _lib.QEDF_ERR_MAXITER}
+    assert torch.equal(out[0][0], out[1][0])
+    assert torch.equal(out[0][1], out[1][1])
+    assert torch.equal(out[0][2], out[1][2])
+    assert _lib.wait_timeouts() == 0
+
+
+@pytest.mark.parametrize("L,Nt,nrhs,slab", [(48, 16, 3, 0), (48, 9, 2, 4), (24, 12, 2, 1), (10, 8, 1, 0)])
+def test_staged_mhm_matches_oracle(L, Nt, nrhs, slab):
+    """Single-precision M^dag M runs the staged engine wherever its shared memory fits."""
+    from qed_fermion_b200 import _lib, ops
+    phi, v = _case(L, Nt, nrhs, seed=3 * L + Nt)
+    phi = phi.reshape(nrhs, -1)
+    v = v.reshape(nrhs, -1)
+    want = O.mhm_vec(phi.reshape(nrhs, Nt, -1), v.reshape(nrhs, Nt, L * L), L, 0.1).reshape(nrhs, -1)
+    got = ops.apply_operator("mhm", torch.tensor(phi, dtype=torch.float32, device=DEV),
+                             torch.tensor(v, dtype=torch.complex64, device=DEV), L, 0.1, slab=slab)
+    g = got.cpu().numpy()
+    assert np.abs(g - want).max() / np.abs(want).max() < 1e-6
+    assert _lib.wait_timeouts() == 0
