@@ -202,6 +202,10 @@ typedef struct {
 #define QEDF_PCG_PLAIN_F64 1 /* complex128 vectors, double angles, double arithmetic */
 #define QEDF_PCG_MIXED 2     /* complex128 b/x, float angles; float iterations with
                                 double reliable updates of x and the true residual */
+#define QEDF_PCG_MIXED_BF16 3 /* as QEDF_PCG_MIXED, with the iteration vectors (r, p, z,
+                                 M^dag M p, the float part of x) stored as bf16 pairs:
+                                 4 bytes per complex number, float arithmetic; lattices
+                                 whose slice stages fit in shared memory (L <= 66) */
 
 typedef struct {
   int mode;           /* QEDF_PCG_* */
@@ -230,9 +234,9 @@ typedef struct {
 /* Bytes of device workspace qedf_pcg_solve needs for these systems. */
 int64_t qedf_pcg_workspace_bytes(const qedf_system* sys, int nsys, const qedf_pcg_opts* opts);
 
-/* Solve.  boson: packed angles (float for PLAIN_F32 / MIXED, double for
- * PLAIN_F64); b, x: packed vectors (complex64 for PLAIN_F32, complex128
- * otherwise); iters, relres, status: device arrays with one entry per
+/* Solve.  boson: packed angles (float for PLAIN_F32 / MIXED / MIXED_BF16,
+ * double for PLAIN_F64); b, x: packed vectors (complex64 for PLAIN_F32,
+ * complex128 otherwise); iters, relres, status: device arrays with one entry per
  * right-hand side (total over systems).  relres is the last measured relative
  * residual (the recomputed true one in MIXED mode).  Returns QEDF_OK when the
  * kernel was launched; per-rhs outcomes are in status. */

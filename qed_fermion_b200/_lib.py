@@ -25,6 +25,7 @@ QEDF_ERR_NAN = 6
 QEDF_PCG_PLAIN_F32 = 0
 QEDF_PCG_PLAIN_F64 = 1
 QEDF_PCG_MIXED = 2
+QEDF_PCG_MIXED_BF16 = 3
 
 
 class QedfSystem(ctypes.Structure):

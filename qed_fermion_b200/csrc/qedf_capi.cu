@@ -182,7 +182,7 @@ int pcg_solve_ws(const qedf_system* sys, int nsys, const void* boson, const void
   if (!boson || !b || !x || !iters || !relres || !status || !workspace) return QEDF_ERR_ARG;
   if (!aligned16(boson) || !aligned16(b) || !aligned16(x) || !aligned16(workspace)) return QEDF_ERR_ARG;
   if (opts->max_iter < 0 || !(opts->rtol >= 0)) return QEDF_ERR_ARG;
-  const int sb = opts->mode == QEDF_PCG_PLAIN_F64 ? 8 : 4;
+  const int sb = pcg_storage_bytes(opts->mode);
   if (ws_bytes < (int64_t)pcg_workspace_bytes(p, sb)) return QEDF_ERR_ARG;
   size_t zero_bytes = 0;
   pcg_carve(p, sb, workspace, &zero_bytes);
@@ -318,7 +318,7 @@ int qedf_wait_timeouts(unsigned int* count) {
 int64_t qedf_pcg_workspace_bytes(const qedf_system* sys, int nsys, const qedf_pcg_opts* opts) {
   PcgParams p;
   if (pcg_plan(p, sys, nsys, opts) != QEDF_OK) return -1;
-  const int sb = opts->mode == QEDF_PCG_PLAIN_F64 ? 8 : 4;
+  const int sb = pcg_storage_bytes(opts->mode);
   return (int64_t)pcg_workspace_bytes(p, sb);
 }
 

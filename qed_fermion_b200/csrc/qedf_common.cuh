@@ -5,8 +5,11 @@
 // pointers of twice the length.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <type_traits>
 
 #include "../../include/qedf.h"
 
@@ -115,6 +118,47 @@ __device__ __forceinline__ void st2(double* p, Cx<double> a, Cx<double> b) {
   reinterpret_cast<double2*>(p)[0] = make_double2(a.re, a.im);
   reinterpret_cast<double2*>(p)[1] = make_double2(b.re, b.im);
 }
+// Storage of single-precision iteration vectors: float (complex64) or bf16
+// pairs (4 bytes per complex number, the BF16 storage option of the PCG).
+// ld2s / st2s move two consecutive complex numbers (16 B as float, 8 B as
+// bf16); arithmetic stays in float.  round_st returns the value the storage
+// keeps (round to nearest even for bf16), so that values kept in registers
+// equal the stored ones.
+using bf16 = __nv_bfloat16;
+__device__ __forceinline__ void ld2s(const float* p, Cx<float>& a, Cx<float>& b) { ld2c(p, a, b); }
+__device__ __forceinline__ void ld2s(const bf16* p, Cx<float>& a, Cx<float>& b) {
+  const uint2 q = *reinterpret_cast<const uint2*>(p);
+  const float2 lo = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&q.x));
+  const float2 hi = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&q.y));
+  a = mk<float>(lo.x, lo.y);
+  b = mk<float>(hi.x, hi.y);
+}
+__device__ __forceinline__ void ld2s(const double* p, Cx<double>& a, Cx<double>& b) { ld2c(p, a, b); }
+__device__ __forceinline__ void st2s(float* p, Cx<float> a, Cx<float> b) { st2(p, a, b); }
+__device__ __forceinline__ void st2s(double* p, Cx<double> a, Cx<double> b) { st2(p, a, b); }
+__device__ __forceinline__ void st2s(bf16* p, Cx<float> a, Cx<float> b) {
+  const __nv_bfloat162 lo = __floats2bfloat162_rn(a.re, a.im);
+  const __nv_bfloat162 hi = __floats2bfloat162_rn(b.re, b.im);
+  uint2 q;
+  q.x = *reinterpret_cast<const unsigned*>(&lo);
+  q.y = *reinterpret_cast<const unsigned*>(&hi);
+  *reinterpret_cast<uint2*>(p) = q;
+}
+template <typename S>
+__device__ __forceinline__ S to_st(double v) {
+  if constexpr (std::is_same<S, bf16>::value) return __float2bfloat16_rn((float)v);
+  else return (S)v;
+}
+template <typename S, typename R>
+__device__ __forceinline__ Cx<R> round_st(Cx<R> v) {
+  if constexpr (std::is_same<S, bf16>::value) {
+    const float2 f = __bfloat1622float2(__floats2bfloat162_rn(v.re, v.im));
+    return mk<R>(f.x, f.y);
+  } else {
+    return v;
+  }
+}
+
 // four reals (angles or forces of two sites, both components)
 __device__ __forceinline__ void ld4(const float* p, float (&a)[4]) {
   float4 q = __ldg(reinterpret_cast<const float4*>(p));
@@ -139,6 +183,12 @@ __device__ __forceinline__ void st4(double* p, const double (&a)[4]) {
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+// 8-byte variant (bf16 pairs of two sites); it allocates in L1 like a plain
+// load, which the grid barrier's acquire makes coherent in the same way
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>

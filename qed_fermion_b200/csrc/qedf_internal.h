@@ -111,7 +111,7 @@ struct PcgSys {
 struct PcgParams {
   int nsys, nrhs, unitsA, unitsE, CH;
   PcgSys sys[PCG_MAX_SYS];
-  int mode;  // QEDF_PCG_PLAIN_F32, QEDF_PCG_PLAIN_F64, QEDF_PCG_MIXED
+  int mode;  // QEDF_PCG_PLAIN_F32, QEDF_PCG_PLAIN_F64, QEDF_PCG_MIXED, QEDF_PCG_MIXED_BF16
   int xs;    // allow the warp-shuffle engine for the single-precision iterations
   int stage; // 1: allow the staged operator engine (EC_STAGE) where its shared memory fits
   int stage_off;  // bytes: start of the operator passes' slice stages in dynamic shared memory
@@ -144,6 +144,8 @@ struct PcgParams {
 
 size_t pcg_workspace_bytes(const PcgParams& p, int sloppy_bytes);
 size_t pcg_carve(PcgParams& p, int sloppy_bytes, void* workspace, size_t* zero_bytes);
+// bytes of one real of the iteration vectors' storage for a QEDF_PCG_* mode
+int pcg_storage_bytes(int mode);
 int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts* o);
 int launch_pcg(PcgParams& p, int by, cudaStream_t st);
 int launch_pcg_prep(const PcgParams& p, int zero_words, cudaStream_t st);

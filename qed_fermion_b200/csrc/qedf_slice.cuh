@@ -53,9 +53,11 @@ struct MaxThreads {
 //   EC_STAGE   the vector slices an operator pass reads are staged whole in
 //              shared memory by bulk copies one slice ahead (SliceStages), so
 //              no thread waits on a global load in the slice loop
+//   EC_BF16    (PCG, with EC_STAGE) the iteration vectors are stored as bf16
+//              pairs; the arithmetic stays in single precision
 //   EC_L(l)    (bits 8 and up) the lattice side fixed at compile time, so the
 //              engine's index arithmetic folds into constants; 0 = run-time L
-enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_STAGE = 8 };
+enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_STAGE = 8, EC_BF16 = 16 };
 __host__ __device__ constexpr int EC_L(int l) { return l << 8; }
 __host__ __device__ constexpr int ec_fixed_l(int ec) { return ec >> 8; }
 // Lattice sides with engines compiled for their size: the benchmark
@@ -204,6 +206,17 @@ struct Slice {
   __device__ __forceinline__ void store(R* slice, const Cx<R> (&v)[BY][2]) const {
 #pragma unroll
     for (int r = 0; r < BY; ++r) st2(slice + 2 * ((y0 + r) * L + x0), v[r][0], v[r][1]);
+  }
+  // the same through a storage type S (float, double or bf16 pairs; see ld2s)
+  template <typename S>
+  __device__ __forceinline__ void load_st(Cx<R> (&v)[BY][2], const S* slice) const {
+#pragma unroll
+    for (int r = 0; r < BY; ++r) ld2s(slice + 2 * ((y0 + r) * L + x0), v[r][0], v[r][1]);
+  }
+  template <typename S>
+  __device__ __forceinline__ void store_st(S* slice, const Cx<R> (&v)[BY][2]) const {
+#pragma unroll
+    for (int r = 0; r < BY; ++r) st2s(slice + 2 * ((y0 + r) * L + x0), v[r][0], v[r][1]);
   }
 
   // thread-private parking of one block (no synchronisation needed)

@@ -11,7 +11,11 @@ Precision modes:
   "fp64"  complex128 vectors, float64 angles, double arithmetic;
   "mixed" complex128 b and x, float32 angles, float iterations with double
           reliable updates (x accumulated and the true residual recomputed in
-          double), so the solution meets rtol down to ~1e-12.
+          double), so the solution meets rtol down to ~1e-12;
+  "mixed_bf16" the same with the iteration vectors (r, p, z, M^dag M p and
+          the float part of x) stored as bf16 pairs, 4 bytes per complex
+          number; the arithmetic stays in float and convergence is still
+          decided on the double-precision true residual.
 """
 from __future__ import annotations
 
@@ -23,9 +27,11 @@ import torch
 from . import _lib
 from .ops import ptr, stream_handle
 
-MODES = {"fp32": _lib.QEDF_PCG_PLAIN_F32, "fp64": _lib.QEDF_PCG_PLAIN_F64, "mixed": _lib.QEDF_PCG_MIXED}
-VEC_DTYPE = {"fp32": torch.complex64, "fp64": torch.complex128, "mixed": torch.complex128}
-ANGLE_DTYPE = {"fp32": torch.float32, "fp64": torch.float64, "mixed": torch.float32}
+MODES = {"fp32": _lib.QEDF_PCG_PLAIN_F32, "fp64": _lib.QEDF_PCG_PLAIN_F64, "mixed": _lib.QEDF_PCG_MIXED,
+         "mixed_bf16": _lib.QEDF_PCG_MIXED_BF16}
+VEC_DTYPE = {"fp32": torch.complex64, "fp64": torch.complex128, "mixed": torch.complex128,
+             "mixed_bf16": torch.complex128}
+ANGLE_DTYPE = {"fp32": torch.float32, "fp64": torch.float64, "mixed": torch.float32, "mixed_bf16": torch.float32}
 
 
 @dataclass(frozen=True)

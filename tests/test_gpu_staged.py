@@ -75,3 +75,27 @@ def test_staged_mhm_matches_oracle(L, Nt, nrhs, slab):
     g = got.cpu().numpy()
     assert np.abs(g - want).max() / np.abs(want).max() < 1e-6
     assert _lib.wait_timeouts() == 0
+
+
+@pytest.mark.parametrize("L,Nt,nrhs,kind", [(12, 40, 2, "piflux"), (48, 48, 2, "piflux"), (20, 14, 1, "piflux")])
+def test_pcg_bf16_storage_meets_rtol_on_true_residual(L, Nt, nrhs, kind):
+    """Vectors stored as bf16 pairs, float arithmetic, double reliable updates:
+    the returned x meets rtol = 1e-10 on the true residual (the oracle's
+    operator on the same angles) and agrees with the oracle's solution."""
+    from qed_fermion_b200.solver import PcgSolver, System
+    phi, b = _case(L, Nt, nrhs, seed=L * Nt)
+    s = PcgSolver([System(L, Nt, nrhs)], mode="mixed_bf16", rtol=1e-10, max_iter=20000, device=DEV,
+                  timeout_ms=500.0)
+    res = s.solve(torch.tensor(phi, dtype=torch.float32, device=DEV), torch.tensor(b, device=DEV))
+    assert res.status.cpu().tolist() == [0] * nrhs
+    x = res.x.cpu().numpy().reshape(nrhs, -1)
+    phi32 = phi.astype(np.float32).astype(np.float64).reshape(nrhs, Nt, -1)
+    bb = b.reshape(nrhs, -1)
+    r = bb - O.mhm_vec(phi32, x.reshape(nrhs, Nt, L * L), L, 0.1).reshape(nrhs, -1)
+    true_rel = np.linalg.norm(r, axis=1) / np.linalg.norm(bb, axis=1)
+    assert np.all(true_rel < 2e-10), true_rel
+    # same system in plain mixed precision: same solution to the solver tolerance
+    m = PcgSolver([System(L, Nt, nrhs)], mode="mixed", rtol=1e-10, max_iter=20000, device=DEV)
+    xm = m.solve(torch.tensor(phi, dtype=torch.float32, device=DEV), torch.tensor(b, device=DEV)).x
+    xm = xm.cpu().numpy().reshape(nrhs, -1)
+    assert np.abs(x - xm).max() / np.abs(xm).max() < 1e-7
