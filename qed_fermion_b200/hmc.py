@@ -37,6 +37,17 @@ def ref_to_kernel(boson: torch.Tensor) -> torch.Tensor:
     return boson.permute(0, 4, 3, 2, 1).reshape(boson.shape[0], -1).contiguous()
 
 
+def metropolis_accept(H_old: torch.Tensor, H_new: torch.Tensor, u: torch.Tensor):
+    """The accept test of ``metropolis_update`` (``hmc_sampler_batch.py:2910``)
+    in double precision: ``u < exp(H_old - H_new)`` per chain, with ``u``
+    uniform in [0, 1).  Returns (accept mask, min(exp(H_old - H_new), 1)), the
+    second being the value each chain's threshold queue records (:2921).  A
+    non-finite Delta H is rejected."""
+    w = torch.exp(H_old.double() - H_new.double())
+    accept = u.double() < w
+    return accept, torch.clamp(torch.nan_to_num(w, nan=0.0), max=1.0)
+
+
 def kernel_to_ref(phi: torch.Tensor, Lx: int, Ltau: int) -> torch.Tensor:
     bs = phi.shape[0]
     return phi.view(bs, Ltau, Lx, Lx, 2).permute(0, 4, 3, 2, 1).contiguous()
@@ -364,9 +375,9 @@ class HmcSampler:
     def _metropolis_step(self, tau_mask):
         boson_new, H_old, H_new, it, err = self.leapfrog_proposer5(self.boson, tau_mask)
         u = torch.rand(self.bs, device=self.device, dtype=torch.float64, generator=self.generator)
-        accp = u < torch.exp(H_old - H_new)
+        accp, thr = metropolis_accept(H_old, H_new, u)
         self.boson = torch.where(accp.view(-1, 1, 1, 1, 1), boson_new.to(self.boson.dtype), self.boson)
-        thresholds = torch.clamp(torch.exp(H_old - H_new), max=1.0).cpu().tolist()
+        thresholds = thr.cpu().tolist()
         for b in range(self.bs):
             self.threshold_queue[b].append(thresholds[b])
         return accp, it, err, H_old, H_new
