@@ -5,6 +5,7 @@ Run where the reference source tree is present, giving its root directory:
     python tests/golden/make_golden.py <reference-root>          # golden_ref.npz, golden_traj.npz
     python tests/golden/make_golden.py <reference-root> bond     # golden_bond.npz
     python tests/golden/make_golden.py <reference-root> fourier  # golden_fourier_mass.npz
+    python tests/golden/make_golden.py <reference-root> mid      # golden_traj_L12.npz
 
 The reference module ``qed_fermion.hmc_sampler_batch`` imports ``matplotlib``
 and ``matlab.engine`` at module level; neither is needed for the CPU path, so
@@ -236,6 +237,36 @@ def gen_trajectory(H, out, rng):
     out["traj_cg_iters_mean"] = its.numpy()
 
 
+def gen_trajectory_mid(H, rng):
+    """A trajectory at the benchmark's step size (20 leapfrog steps of 0.05)
+    on a mid-size lattice, L = 12, Ltau = 120, from the reference's physical
+    start (staggered pi-flux plus noise), PCG to 1e-10."""
+    import torch
+    L, Nt = 12, 120
+    hmc = make_sampler(H, L, Nt)
+    hmc.cg_rtol = 1e-10
+    hmc.max_iter = 50000
+    hmc.N_leapfrog = 20
+    hmc.delta_t_tensor = torch.full((1,), 0.05, dtype=torch.float64)
+    b = pi_flux_boson(rng, L, Nt, noise=0.05)
+    p0 = rng.standard_normal((1, 2, L, L, Nt))
+    R = cvec(rng, L * L * Nt)[None, :] / math.sqrt(2)
+    hmc.draw_momentum = lambda: torch.tensor(p0, dtype=torch.float64)
+    hmc.draw_psudo_fermion = lambda: torch.tensor(R, dtype=torch.complex128)
+    tau_mask = torch.ones((1, 1, 1, 1, Nt), dtype=torch.float64)
+    x, H0, H_fin, its, errs = hmc.leapfrog_proposer5(torch.tensor(b, dtype=torch.float64), tau_mask)
+    return {"mid_boson": b, "mid_p0": p0, "mid_R": R, "mid_x": x.numpy(), "mid_H0": H0.numpy(),
+            "mid_Hfin": H_fin.numpy(), "mid_delta_t": np.array(0.05), "mid_n_leapfrog": np.array(20),
+            "mid_cg_iters_mean": its.numpy()}
+
+
+def main_mid(ref_root):
+    H, _ = import_reference(ref_root)
+    out = gen_trajectory_mid(H, np.random.default_rng(20261204))
+    np.savez_compressed(os.path.join(HERE, "golden_traj_L12.npz"), **out)
+    print("wrote", sorted(out))
+
+
 def gen_estimator(H, out, rng):
     import torch
     L, Nt, nrv = 4, 10, 6
@@ -367,5 +398,7 @@ if __name__ == "__main__":
         main_bond(sys.argv[1])
     elif len(sys.argv) > 2 and sys.argv[2] == "fourier":
         main_fourier(sys.argv[1])
+    elif len(sys.argv) > 2 and sys.argv[2] == "mid":
+        main_mid(sys.argv[1])
     else:
         main()

@@ -1,7 +1,7 @@
 """The staged operator engine (input slices copied whole into shared memory by
 bulk copies, one slice ahead) against the engine that loads them directly:
-the same arithmetic on the same values, so the PCG results agree bit for bit,
-and the staged M^dag M against the oracle."""
+the same arithmetic on the same values, so the PCG solutions agree bit for bit,
+and the staged M^dag M against the oracle; also the bf16 vector storage mode."""
 import numpy as np
 import pytest
 import torch
@@ -58,7 +58,9 @@ def test_pcg_staged_engine_is_bit_identical(mode, systems):
     assert set(out[0][3].cpu().tolist()) <= {0, _lib.QEDF_ERR_MAXITER}
     assert torch.equal(out[0][0], out[1][0])
     assert torch.equal(out[0][1], out[1][1])
-    assert torch.equal(out[0][2], out[1][2])
+    # the residual norms are double sums that blocks add atomically in a
+    # run-dependent order, so they agree to rounding rather than bit for bit
+    assert torch.allclose(out[0][2], out[1][2], rtol=1e-12, atol=0)
     assert _lib.wait_timeouts() == 0
 
 
