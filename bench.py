@@ -59,7 +59,16 @@ def parse_args(argv=None):
     ap.add_argument("--n-leapfrog", type=int, default=20)
     ap.add_argument("--delta-t", type=float, default=0.05)
     ap.add_argument("--rtol", type=float, default=1e-10)
-    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--fp64-steps", type=int, default=5, help="trajectories timed on the plain FP64 path")
+    ap.add_argument("--bf16-steps", type=int, default=5,
+                    help="trajectories timed with the PCG's vectors stored as bf16 (mixed arithmetic)")
+    ap.add_argument("--dropin-steps", type=int, default=1,
+                    help="trajectories of the reference's per-iteration loop on the _C kernels (complex128)")
+    ap.add_argument("--accept-steps", type=int, default=20,
+                    help="Metropolis steps of the acceptance comparison, mixed against FP64")
+    ap.add_argument("--accept-delta-t", type=float, default=0.002,
+                    help="leapfrog step of the acceptance comparison: at the headline step 0.05 Delta H is "
+                         "about 500 on this lattice and nothing is accepted")
     ap.add_argument("--mhm-rhs", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--cg-iters-per-solve", type=float, default=None,
@@ -78,7 +87,7 @@ def parse_args(argv=None):
                     help="time the other benchmark configurations (C2, C4a, C4b, C5), one JSON line each")
     ap.add_argument("--matvec-only", type=int, default=0,
                     help="only time M^dag M on this many right-hand sides (c64; c128 with --mode fp64)")
-    ap.add_argument("--mode", default="mixed", choices=["mixed", "fp32", "fp64"],
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "mixed_bf16", "fp32", "fp64"],
                     help="precision of the --solve-only solve or --matvec-only launch")
     ap.add_argument("--quick", action="store_true",
                     help="timed trajectories only (no e2e, FP64, Delta H, matvec or CPU legs): for profiling")
@@ -443,7 +452,7 @@ def run_native(args):
         hb.copy_(hmc.boson.cpu())
         hout = torch.empty_like(hb).pin_memory()
         hH = torch.empty((3, bs), dtype=torch.float64, pin_memory=True)
-        k_e2e = max(1, min(args.steps, 2))
+        k_e2e = args.steps
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -461,56 +470,108 @@ def run_native(args):
         e2e = {"value": 3600.0 * k_e2e * bs / t_e2e, "unit": UNIT, "h2d_bytes_per_step": hb.numel() * 4,
                "d2h_bytes_per_step": hout.numel() * 4 + hH.numel() * 8, "steps": k_e2e}
 
+    def time_trajectories(h, n):
+        h.metropolis_update()  # warm-up
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        its = []
+        e0.record(stream)
+        for _ in range(n):
+            _, _, it, _, _, _ = h.metropolis_update()
+            its.append(it)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3
+        return {"value": 3600.0 * n * bs / t, "unit": UNIT, "steps": n, "s_per_trajectory": t / n,
+                "cg_iters_per_solve": float(torch.stack(its).double().mean())}
+
     # --- plain FP64 path, same workload
     fp64 = None
     if rank == 0 and args.fp64_steps > 0 and not args.quick:
         h64 = make("fp64")
         h64.boson = hmc.boson.to(torch.float64)
-        h64.metropolis_update()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.fp64_steps):
-            h64.metropolis_update()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        t64 = e0.elapsed_time(e1) / 1e3
-        fp64 = {"value": 3600.0 * args.fp64_steps * bs / t64, "unit": UNIT, "steps": args.fp64_steps,
-                "s_per_trajectory": t64 / args.fp64_steps,
-                "path": "same engine in double (persistent PCG, double force)"}
-        # the drop-in path: the reference's per-iteration PCG loop on this library's
-        # _C kernels in complex128 (one trajectory, same workload)
-        hd = make("fp64", solver_impl="reference_loop")
-        hd.boson = hmc.boson.to(torch.float64)
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        hd.metropolis_update()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        td = e0.elapsed_time(e1) / 1e3
-        fp64["dropin"] = {"value": 3600.0 * bs / td, "unit": UNIT, "steps": 1, "s_per_trajectory": td,
-                          "path": "reference loop structure (preconditioned_cg_fast_test) on _C kernels, "
-                                  "complex128"}
+        fp64 = time_trajectories(h64, args.fp64_steps)
+        fp64["path"] = "same engine in double (persistent PCG, double force)"
+        del h64
+        if args.dropin_steps > 0:
+            # the drop-in path: the reference's per-iteration PCG loop on this library's
+            # _C kernels in complex128, same workload
+            hd = make("fp64", solver_impl="reference_loop")
+            hd.boson = hmc.boson.to(torch.float64)
+            fp64["dropin"] = time_trajectories(hd, args.dropin_steps)
+            fp64["dropin"]["path"] = ("reference loop structure (preconditioned_cg_fast_test) on _C kernels, "
+                                      "complex128")
+            del hd
 
-    # --- Delta H of one shared trajectory, mixed vs FP64
+    # --- bf16 vector storage, same workload
+    bf16 = None
+    if rank == 0 and args.bf16_steps > 0 and not args.quick:
+        hb16 = make("mixed_bf16")
+        hb16.boson = hmc.boson.clone()
+        bf16 = time_trajectories(hb16, args.bf16_steps)
+        bf16["path"] = "mixed precision with the PCG's vectors stored as bf16 pairs"
+        bf16["pcg_bytes_per_site_iteration"] = 7 * 4 + 2 * 4
+        del hb16
+
+    # --- Delta H of one shared trajectory: mixed and bf16 storage against FP64
     dH = None
     if rank == 0 and not args.quick:
-        h64 = make("fp64")
         gen = torch.Generator(device=dev)
         gen.manual_seed(seed + 7)
         x0 = hmc.boson.to(torch.float64)
         p0 = torch.randn(x0.shape, device=dev, dtype=torch.float64, generator=gen)
         R = torch.randn((bs, N), device=dev, dtype=torch.complex128, generator=gen) / math.sqrt(2)
-        _, H0m, H1m, _, _ = hmc.leapfrog_proposer5(x0.to(torch.float32), p0=p0.to(torch.float32), R=R)
+        h64 = make("fp64")
         _, H0d, H1d, _, _ = h64.leapfrog_proposer5(x0.to(torch.float32).to(torch.float64),
                                                     p0=p0.to(torch.float32).to(torch.float64), R=R)
-        dHm, dHd = (H1m - H0m).cpu(), (H1d - H0d).cpu()
-        dH = {"dH_mixed": dHm.tolist(), "dH_fp64": dHd.tolist(),
-              "abs_err": (dHm - dHd).abs().tolist(),
-              "rel_err_vs_H0": ((dHm - dHd).abs() / H0d.abs().cpu()).tolist(), "H0": H0d.cpu().tolist()}
+        del h64
+        dHd = (H1d - H0d).cpu()
+        dH = {"dH_fp64": dHd.tolist(), "H0": H0d.cpu().tolist()}
+        for name, h in (("mixed", hmc), ("mixed_bf16", make("mixed_bf16"))):
+            _, H0m, H1m, _, _ = h.leapfrog_proposer5(x0.to(torch.float32), p0=p0.to(torch.float32), R=R)
+            dHm = (H1m - H0m).cpu()
+            dH[name] = {"dH": dHm.tolist(), "abs_err": (dHm - dHd).abs().tolist(),
+                        "rel_err_vs_H0": ((dHm - dHd).abs() / H0d.abs().cpu()).tolist(),
+                        "rel_err_vs_dH": ((dHm - dHd).abs() / dHd.abs()).tolist()}
+
+    # --- acceptance, mixed against FP64, at a step where proposals are accepted:
+    # both chains take the same momenta, pseudofermions and uniforms each step
+    acc = None
+    if rank == 0 and args.accept_steps > 0 and not args.quick:
+        from qed_fermion_b200.hmc import metropolis_accept
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(seed + 11)
+        hm = make("mixed")
+        hd = make("fp64")
+        hm.delta_t_tensor.fill_(args.accept_delta_t)
+        hd.delta_t_tensor.fill_(args.accept_delta_t)
+        xm = hmc.boson.to(torch.float32).clone()
+        xd = xm.to(torch.float64)
+        rec = {"mixed": [], "fp64": []}
+        nmis, dd = 0, []
+        for _ in range(args.accept_steps):
+            p0 = torch.randn(xd.shape, device=dev, dtype=torch.float64, generator=gen).to(torch.float32)
+            R = torch.randn((bs, N), device=dev, dtype=torch.complex128, generator=gen) / math.sqrt(2)
+            u = torch.rand(bs, device=dev, dtype=torch.float64, generator=gen)
+            nm, H0m, H1m, _, _ = hm.leapfrog_proposer5(xm, p0=p0, R=R)
+            nd, H0d, H1d, _, _ = hd.leapfrog_proposer5(xd, p0=p0.to(torch.float64), R=R)
+            am, _ = metropolis_accept(H0m, H1m, u)
+            ad, _ = metropolis_accept(H0d, H1d, u)
+            xm = torch.where(am.view(-1, 1, 1, 1, 1), nm.to(torch.float32), xm)
+            xd = torch.where(ad.view(-1, 1, 1, 1, 1), nd.to(torch.float64), xd)
+            rec["mixed"].append(((H1m - H0m).cpu(), am.cpu()))
+            rec["fp64"].append(((H1d - H0d).cpu(), ad.cpu()))
+            nmis += int((am != ad).sum())
+            dd.append(((H1m - H0m) - (H1d - H0d)).abs().cpu())
+        acc = {"delta_t": args.accept_delta_t, "n_leapfrog": args.n_leapfrog, "steps": args.accept_steps,
+               "chains": bs, "decisions_differing": nmis,
+               "max_abs_dH_difference": float(torch.stack(dd).max())}
+        for k, v in rec.items():
+            d = torch.stack([a for a, _ in v]).double()
+            acc[k] = {"acceptance": float(torch.stack([b for _, b in v]).double().mean()),
+                      "mean_exp_minus_dH": float(torch.exp(-d).mean()), "mean_dH": float(d.mean())}
+        del hm, hd
 
     # --- M^dag M matvec bandwidth (several right-hand sides, working set > L2)
     mhm = None
@@ -567,8 +628,10 @@ def run_native(args):
                          "bytes_model": "per PCG iteration per rhs: N*(7*8 + 2*4) B (read p,x,r,angles; write x,r,p)"},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "fp64_plain": fp64, "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
-            "speedup_vs_fp64_dropin": (value / world) / fp64["dropin"]["value"] if fp64 else None,
-            "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate, **result,
+            "speedup_vs_fp64_dropin": ((value / world) / fp64["dropin"]["value"]
+                                       if fp64 and "dropin" in fp64 else None),
+            "bf16": bf16, "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate,
+            "acceptance_vs_fp64": acc, **result,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -605,9 +668,11 @@ def run_solve_only(args):
     ms = e0.elapsed_time(e1)
     it = int(res.iters.max())
     n = L * L * Lt * bs
+    # bytes per site and iteration: 7 vector accesses and the two angles
+    bps = {"mixed": 64, "fp32": 64, "fp64": 128, "mixed_bf16": 36}[args.mode]
     print(json.dumps({"solve_only": True, "mode": args.mode, "lattice": [L, L, Lt], "rhs": bs, "iters": it,
-                      "ms": ms, "us_per_iter": ms * 1e3 / max(it, 1),
-                      "algorithmic_GBps": n * 64 * it / (ms / 1e3) / 1e9}), flush=True)
+                      "ms": ms, "us_per_iter": ms * 1e3 / max(it, 1), "bytes_per_site_iter": bps,
+                      "algorithmic_GBps": n * bps * it / (ms / 1e3) / 1e9}), flush=True)
     return 0
 
 

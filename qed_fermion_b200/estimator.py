@@ -20,7 +20,7 @@ from .solver import PcgSolver, System
 
 class StochaticEstimator:
     def __init__(self, Lx, Ltau, Nrv=20, dtau=0.1, precision="mixed", cg_rtol=1e-10, max_iter=20000,
-                 use_precon=True, device=None, seed=None, noise="z2z2"):
+                 use_precon=True, device=None, seed=None, noise="z2z2", autotune=True):
         self.Lx, self.Ly, self.Ltau, self.Nrv, self.dtau = Lx, Lx, Ltau, Nrv, dtau
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         self.noise = noise
@@ -29,7 +29,8 @@ class StochaticEstimator:
             self.generator.manual_seed(seed)
         mode = precision
         self.solver = PcgSolver([System(Lx, Ltau, Nrv, True)], mode=mode, rtol=cg_rtol, max_iter=max_iter,
-                                dtau=dtau, use_precon=use_precon and Ltau >= 26, device=self.device)
+                                dtau=dtau, use_precon=use_precon and Ltau >= 26, device=self.device,
+                                tune=autotune)
         self.eta = None
         self.G_eta = None
 

@@ -58,7 +58,7 @@ class HmcSampler:
     def __init__(self, Lx=6, Ltau=10, J=1.0, K=1.0, dtau=0.1, bs=1, delta_t=0.06, N_leapfrog=5, m=1.0,
                  compact=False, precision="mixed", cg_rtol=1e-10, max_iter=20000, use_precon=True,
                  ru_interval=50, ru_delta=0.1, device=None, seed=None, solver_impl="persistent",
-                 max_tau_block_idx=1):
+                 max_tau_block_idx=1, autotune=True):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}")
         if Lx % 2:
@@ -90,7 +90,7 @@ class HmcSampler:
         solver_mode = {"fp64": "fp64", "mixed": "mixed", "mixed_bf16": "mixed_bf16", "fp32": "fp32"}[precision]
         self.solver = PcgSolver([System(Lx, Ltau, bs, False)], mode=solver_mode, rtol=cg_rtol, max_iter=max_iter,
                                 dtau=dtau, use_precon=self.use_precon, ru_interval=ru_interval,
-                                ru_delta=ru_delta, device=self.device)
+                                ru_delta=ru_delta, device=self.device, tune=autotune)
         # "persistent": one cooperative PCG kernel per solve; "reference_loop": the
         # reference's per-iteration launch sequence (preconditioned_cg_fast_test) on
         # this library's _C kernels -- the drop-in path

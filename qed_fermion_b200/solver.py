@@ -68,6 +68,10 @@ class PcgSolver:
     set-aside as it is (the limit is never changed), and releases the window's
     lines after the solve.  Pass False for no window.
 
+    ``tune`` takes ``by``, ``slab`` and ``stage`` from the autotuner
+    (:mod:`qed_fermion_b200.autotune`), which times the candidates once per
+    problem shape and caches the winner; explicit ``by`` / ``slab`` win over it.
+
     ``stage`` (default on) lets the single-precision operator passes stage
     their input slices in shared memory by bulk copies where the stages fit;
     False selects the engine that loads them directly (the results are the
@@ -78,12 +82,19 @@ class PcgSolver:
                  max_iter: int = 10000, dtau: float = 0.1, use_precon: bool = True,
                  ru_interval: int = 50, ru_delta: float = 0.1, by: int = 0, slab: int = 0,
                  chunk: int = 0, timeout_ms: float = 2000.0, profile: bool = False, device=None,
-                 l2_persist: bool = True, stage: bool = True):
+                 l2_persist: bool = True, stage: bool = True, tune: bool = False):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {sorted(MODES)}")
         self.systems = [s if isinstance(s, System) else System(*s) for s in systems]
         self.mode = mode
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        # launch shape: explicit, or timed once per shape by the autotuner
+        self.tuned = None
+        if tune and by == 0 and slab == 0 and self.device.type == "cuda":
+            from . import autotune
+            with torch.cuda.device(self.device):
+                self.tuned = autotune.pcg_choice(self.systems, mode, use_precon=use_precon, dtau=dtau)
+            by, slab, stage = self.tuned["by"], self.tuned["slab"], self.tuned["stage"]
         n = len(self.systems)
         self._sys = (_lib.QedfSystem * n)(*[_lib.QedfSystem(s.Lx, s.Ltau, s.nrhs, 1 if s.shared_boson else 0)
                                             for s in self.systems])
