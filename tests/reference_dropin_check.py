@@ -45,6 +45,7 @@ def main(ref_dir, repo):
     from qed_fermion.stochastic_estimator import StochaticEstimator
     from oracle import qedf_oracle as O
     assert H._C is qed_fermion_b200._C, "the reference did not bind the drop-in _C"
+    H.Nstep = 4  # a module global the reference's __main__ block defines and its sampler reads
     # the reference writes its preconditioner file next to its sources; keep it in a temp dir
     tmp = tempfile.mkdtemp(prefix="qedf_dropin_")
     H.script_path = tmp
