@@ -176,6 +176,40 @@ int qedf_bb_kspace_acc_c128(const double* A, const double* B, int64_t rows, int 
                             qedf_stream_t stream);
 
 /* ---------------------------------------------------------------------------
+ * Adaptive Fourier mass of the boson momenta (hmc_sampler_batch.py:1133-1277):
+ * the arithmetic around the real FFTs over [Lx][Ly][Ltau] (the FFTs
+ * themselves are the caller's).  Arrays are per (chain, direction) rows.
+ *
+ * qedf_fm_accumulate: mean = (cnt mean + x) / (cnt + 1), d = x - mean
+ *   (update_sigma_hat_cpu :1202-1207, its running mean; n reals).
+ * qedf_fm_spectrum: S = (cnt S + |X|^2) / (cnt + 1) for the orthonormal
+ *   transform X of d (:1208-1210; n complex X, n real S).
+ * qedf_fm_mass: per row of len values, sigma = the mass spectrum of S:
+ *   clamp to [0, *clamp_hi], Box-Cox (exponent lambda), rescale into
+ *   [smin, smax], shift the row mean to 1, shrink towards 1 by lmd, invert if
+ *   invert != 0 (apply_sigma_hat_cpu :1133-1200; *clamp_hi is the mean over
+ *   rows of the rows' 0.99 quantiles, a device scalar).  sigma may alias S.
+ * qedf_fm_noise: z = (a + i b) / sqrt(sigma m_k), m_k = 1 for the first and
+ *   last of the nk tau frequencies, else 2 (draw_momentum_fft :1254-1265).
+ * qedf_fm_scale: P = P sigma, complex P times real sigma (apply_m_inv
+ *   :1267-1277).
+ * ------------------------------------------------------------------------- */
+int qedf_fm_accumulate_f32(float* mean, const float* x, float* d, int64_t n, double cnt, qedf_stream_t stream);
+int qedf_fm_accumulate_f64(double* mean, const double* x, double* d, int64_t n, double cnt, qedf_stream_t stream);
+int qedf_fm_spectrum_f32(float* S, const float* X, int64_t n, double cnt, qedf_stream_t stream);
+int qedf_fm_spectrum_f64(double* S, const double* X, int64_t n, double cnt, qedf_stream_t stream);
+int qedf_fm_mass_f32(const float* S, float* sigma, int rows, int64_t len, const float* clamp_hi, double lambda,
+                     double smin, double smax, double lmd, int invert, qedf_stream_t stream);
+int qedf_fm_mass_f64(const double* S, double* sigma, int rows, int64_t len, const double* clamp_hi, double lambda,
+                     double smin, double smax, double lmd, int invert, qedf_stream_t stream);
+int qedf_fm_noise_f32(const float* a, const float* b, const float* sigma, float* z, int64_t n, int nk,
+                      qedf_stream_t stream);
+int qedf_fm_noise_f64(const double* a, const double* b, const double* sigma, double* z, int64_t n, int nk,
+                      qedf_stream_t stream);
+int qedf_fm_scale_f32(float* P, const float* sigma, int64_t n, qedf_stream_t stream);
+int qedf_fm_scale_f64(double* P, const double* sigma, int64_t n, qedf_stream_t stream);
+
+/* ---------------------------------------------------------------------------
  * Batched preconditioned CG on M^dag M x = b (persistent kernel).
  *
  * Replaces preconditioned_cg_fast_test (hmc_sampler_batch.py:751-846) and the

@@ -712,3 +712,51 @@ def bb_observables(eta, G, boson, L, Nt):
 
 def bb_bond_corr(BB_r_mean, B_r_mean):
     return BB_r_mean - 4 * _corr(B_r_mean, B_r_mean)
+
+
+# ----------------------------------------------------------------------------
+# adaptive Fourier mass (hmc_sampler_batch.py:1133-1277)
+# ----------------------------------------------------------------------------
+
+
+def fm_accumulate(mean, spec, field, cnt):
+    """One step of the running statistics (``update_sigma_hat_cpu`` :1202-1210):
+    the field mean and the mean power spectrum of the centred field under the
+    orthonormal real FFT over the last three axes, each averaged over the
+    ``cnt + 1`` steps of the window.  Returns (mean, spec)."""
+    mean = (mean * cnt + field) / (cnt + 1)
+    X = np.fft.rfftn(field - mean, axes=(-3, -2, -1), norm="ortho")
+    return mean, (spec * cnt + np.abs(X) ** 2) / (cnt + 1)
+
+
+def fm_mass(spec, lam=0.05, smin=0.8, smax=1.2, lmd=0.9, invert=False):
+    """The mass spectrum from the accumulated spectrum (``apply_sigma_hat_cpu``
+    :1133-1200) for ``spec`` of shape [bs, 2, ...]: clamp to [0, c] with c the
+    mean over (chain, direction) rows of the rows' 0.99 quantiles; Box-Cox
+    (s^lam - 1) / lam; per row, rescale into [smin, smax] and shift the mean
+    to 1; shrink towards 1 by lmd; invert for mass mode -1."""
+    rows = spec.reshape(spec.shape[0] * spec.shape[1], -1)
+    c = np.quantile(rows, 0.99, axis=-1).mean()
+    s = (np.clip(rows, 0.0, c) ** lam - 1.0) / lam
+    lo = s.min(axis=-1, keepdims=True)
+    hi = s.max(axis=-1, keepdims=True)
+    s = (s - lo) / np.maximum(hi - lo, 1e-8) * (smax - smin) + smin
+    s = s - s.mean(axis=-1, keepdims=True) + 1.0
+    s = (1.0 - lmd) * s + lmd
+    if invert:
+        s = 1.0 / s
+    return s.reshape(spec.shape)
+
+
+def fm_draw(sigma, a, b, shape):
+    """Momenta with the Fourier mass (``draw_momentum_fft`` :1254-1265): the
+    inverse orthonormal real FFT of (a + i b) / sqrt(sigma m_k), m_k = 1 for
+    the first and last tau frequency and 2 otherwise."""
+    m = np.full(sigma.shape[-1], 2.0)
+    m[[0, -1]] = 1.0
+    return np.fft.irfftn((a + 1j * b) / np.sqrt(sigma * m), s=shape, axes=(-3, -2, -1), norm="ortho")
+
+
+def fm_m_inv(p, sigma):
+    """``M^-1 p = F^-1 (sigma F p)`` (``apply_m_inv`` :1267-1277, unnormalised FFT pair)."""
+    return np.fft.irfftn(np.fft.rfftn(p, axes=(-3, -2, -1)) * sigma, s=p.shape[-3:], axes=(-3, -2, -1))

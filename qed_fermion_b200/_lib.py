@@ -73,6 +73,13 @@ for _r in ("f32", "f64"):
         c_int, [_vp, _vp, _vp, c_int, c_int, c_int, c_double, c_double, c_int, c_double, _vp])
     SIGNATURES[f"qedf_kick_drift_{_r}"] = (
         c_int, [_vp, _vp, _vp, _vp, _vp, c_double, c_double, c_int, c_int, c_int, _vp])
+for _r in ("f32", "f64"):
+    SIGNATURES[f"qedf_fm_accumulate_{_r}"] = (c_int, [_vp, _vp, _vp, c_int64, c_double, _vp])
+    SIGNATURES[f"qedf_fm_spectrum_{_r}"] = (c_int, [_vp, _vp, c_int64, c_double, _vp])
+    SIGNATURES[f"qedf_fm_mass_{_r}"] = (
+        c_int, [_vp, _vp, c_int, c_int64, _vp, c_double, c_double, c_double, c_double, c_int, _vp])
+    SIGNATURES[f"qedf_fm_noise_{_r}"] = (c_int, [_vp, _vp, _vp, _vp, c_int64, c_int, _vp])
+    SIGNATURES[f"qedf_fm_scale_{_r}"] = (c_int, [_vp, _vp, c_int64, _vp])
 SIGNATURES["qedf_wait_timeouts"] = (c_int, [POINTER(ctypes.c_uint)])
 SIGNATURES["qedf_precon_tau_csr"] = (c_int, [c_int, POINTER(c_int), POINTER(c_int), POINTER(c_double),
                                               POINTER(c_int)])

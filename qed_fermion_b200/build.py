@@ -8,7 +8,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libqedf.so")
-SOURCES = ["qedf_ops.cu", "qedf_pcg.cu", "qedf_capi.cu", "qedf_static.cu", "qedf_bond.cu"]
+SOURCES = ["qedf_ops.cu", "qedf_pcg.cu", "qedf_capi.cu", "qedf_static.cu", "qedf_bond.cu", "qedf_fmass.cu"]
 HEADERS = ["qedf_common.cuh", "qedf_slice.cuh", "qedf_internal.h", "qedf_precon_table.h"]
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-diag-suppress", "20013,20015"]

@@ -1,110 +1,123 @@
-"""Fourier-space adaptive mass of the boson momenta.
+"""Adaptive Fourier mass of the boson momenta (``hmc_sampler_batch.py:1133-1277``).
 
-The reference keeps, per chain and bond direction, a spectrum sigma_hat over
-the rfft grid ``[bs, 2, Lx, Ly, Ltau // 2 + 1]`` (``hmc_sampler_batch.py``
-:272-285).  Every step it accumulates the running mean of |rfftn(boson -
-mean)|^2 (``update_sigma_hat_cpu`` :1202-1210).  Every ``sigma_mini_batch_size``
-steps it turns that spectrum into a mass:
-- clamp at the 0.99 quantile;
-- a Box-Cox transform with lambda = 0.05;
-- rescale into [sig_min, sig_max];
-- shift the mean to 1;
-- shrink towards 1 by lmd;
-- and, in mass mode -1, invert (``apply_sigma_hat_cpu`` :1133-1200).
+Per chain and bond direction the sampler estimates the power spectrum of the
+field's fluctuations on the real-FFT grid ``[Lx, Ly, Ltau // 2 + 1]`` and
+turns it into a mass per mode; momenta drawn with that mass, and the inverse
+mass applied to them, move the slow modes faster.  The arithmetic around the
+FFTs runs in this library's kernels (``qedf_fm_*``), the FFTs are cuFFT's
+through torch, and the statistics stay on the device:
 
-``draw_momentum_fft`` (:1254-1265) and ``apply_m_inv`` (:1267-1277) draw
-momenta with that mass and apply its inverse.  Their call sites in the
-reference's leapfrog are commented out, so the sampler's trajectories do not
-depend on it.  The routines are provided with the reference's names,
-arguments and arithmetic.  FFTs are cuFFT's through torch; the statistics
-live on the CPU, as in the reference.
+* ``update(boson, i)``: the running mean of the field and of the orthonormal
+  power spectrum of the centred field, averaged over a window that restarts
+  at every ``annealing_step``-th step while restarts remain (10 of them);
+* ``apply(i)``: every ``sigma_mini_batch_size`` steps the spectrum becomes
+  the mass spectrum ``sigma_hat`` (clamp at the mean row 0.99 quantile,
+  Box-Cox with ``lambda_``, rescale each row into ``[sig_min, sig_max]``,
+  shift its mean to 1, shrink towards 1 by ``lmd``; inverted for
+  ``mass_mode == -1``);
+* ``draw_momentum_fft`` and ``apply_m_inv``.
+
+The reference's method names (``update_sigma_hat_cpu``,
+``apply_sigma_hat_cpu``) are kept as aliases; its leapfrog does not call the
+draw or M^-1 (those call sites are commented out), so trajectories do not
+depend on this module.
 """
 from __future__ import annotations
 
 import torch
 
+from . import _lib
+from .ops import ptr, stream_handle
+
 
 class FourierMass:
     def __init__(self, bs, Lx, Ltau, dtype=torch.float32, device=None, sigma_mini_batch_size=1000, lmd=0.9,
                  lambda_=0.05, sig_min=0.8, sig_max=1.2, mass_mode=0):
-        self.bs, self.Lx, self.Ly, self.Ltau = bs, Lx, Lx, Ltau
         self.device = torch.device(device) if device is not None else torch.device("cuda")
-        shape = (bs, 2, Lx, Lx, Ltau // 2 + 1)
-        self.sigma_hat = torch.ones(shape, device=self.device, dtype=dtype)
-        self.sigma_hat_cpu = torch.ones(shape, dtype=dtype)
-        self.boson_mean_cpu = torch.zeros((bs, 2, Lx, Lx, Ltau), dtype=dtype)
+        if self.device.type != "cuda":
+            raise RuntimeError("FourierMass runs on the GPU kernels (no CPU fallback)")
+        if dtype not in (torch.float32, torch.float64):
+            raise ValueError("dtype must be float32 or float64")
+        self.bs, self.Lx, self.Ly, self.Ltau = bs, Lx, Lx, Ltau
+        self.dtype = dtype
+        self.grid = (Lx, Lx, Ltau)
+        self.nk = Ltau // 2 + 1
+        kshape = (bs, 2, Lx, Lx, self.nk)
+        self.sigma_hat = torch.ones(kshape, device=self.device, dtype=dtype)
+        self.spectrum = torch.ones(kshape, device=self.device, dtype=dtype)
+        self.field_mean = torch.zeros((bs, 2, Lx, Lx, Ltau), device=self.device, dtype=dtype)
         self.sigma_mini_batch_size = sigma_mini_batch_size
-        self.sigma_hat_mini_batch_last_i = 0
         self.annealing_step = max(50, sigma_mini_batch_size)
-        self.anneal_times = 10
-        # the non-redundant rfft modes along tau count twice, k = 0 and Nyquist once
-        self.multiplier = torch.full_like(self.sigma_hat, 2)
-        self.multiplier[..., torch.tensor([0, -1], device=self.device)] = 1
+        self.restarts_left = 10
+        self.window_start = 0
         self.lmd, self.lambda_, self.sig_min, self.sig_max = lmd, lambda_, sig_min, sig_max
         self.mass_mode = mass_mode
+        self._sfx = "f32" if dtype == torch.float32 else "f64"
 
-    def update_sigma_hat_cpu(self, boson_cpu, i):
-        """Fold step i's field (reference layout, on the CPU) into the running
-        mean and the running mean spectrum; restart the window at each
-        annealing step while annealing steps remain."""
-        if i % self.annealing_step == 0 and i > 0 and self.anneal_times > 0:
-            self.sigma_hat_mini_batch_last_i = i
-            self.anneal_times -= 1
-        cnt = i - self.sigma_hat_mini_batch_last_i
-        self.boson_mean_cpu = (self.boson_mean_cpu * cnt + boson_cpu) / (cnt + 1)
-        d = torch.fft.rfftn(boson_cpu - self.boson_mean_cpu, (self.Lx, self.Ly, self.Ltau), norm="ortho").abs() ** 2
-        self.sigma_hat_cpu = (self.sigma_hat_cpu * cnt + d) / (cnt + 1)
+    # ---- running statistics -------------------------------------------------
+    def update(self, boson, i):
+        """Fold step ``i``'s field (reference layout ``[bs, 2, Lx, Ly, Ltau]``)
+        into the running mean and the running mean spectrum."""
+        if i % self.annealing_step == 0 and i > 0 and self.restarts_left > 0:
+            self.window_start = i
+            self.restarts_left -= 1
+        cnt = float(i - self.window_start)
+        x = boson.to(device=self.device, dtype=self.dtype).contiguous()
+        d = torch.empty_like(x)
+        _lib.call(f"qedf_fm_accumulate_{self._sfx}", ptr(self.field_mean), ptr(x), ptr(d), x.numel(), cnt,
+                  stream_handle())
+        X = torch.fft.rfftn(d, self.grid, norm="ortho").contiguous()
+        _lib.call(f"qedf_fm_spectrum_{self._sfx}", ptr(self.spectrum), ptr(torch.view_as_real(X)),
+                  self.spectrum.numel(), cnt, stream_handle())
 
-    def stabilize_sigma_hat(self, method="shrink", **kw):
-        if method == "shrink":
-            lmd = kw.get("lmd", 0.8)
-            self.sigma_hat = (1 - lmd) * self.sigma_hat + lmd * torch.ones_like(self.sigma_hat)
-        elif method == "pow":
-            self.sigma_hat = self.sigma_hat.pow(kw.get("beta", 0.5))
-        elif method == "clamp":
-            self.sigma_hat = self.sigma_hat.clamp(kw.get("sgm_min", 0.5), kw.get("sgm_max", 2.0))
-        elif method == "clamp_shrink":
-            sgm_min, sgm_max = kw.get("sgm_min", 0.5), kw.get("sgm_max", 2.0)
-            mx = self.sigma_hat.amax(dim=(2, 3, 4), keepdim=True)
-            mn = self.sigma_hat.amin(dim=(2, 3, 4), keepdim=True)
-            self.sigma_hat = torch.where(self.sigma_hat > 1, 1 + (self.sigma_hat - 1) * ((sgm_max - 1) / (mx - 1)),
-                                         1 - (1 - self.sigma_hat) * ((sgm_min - 1) / (mn - 1)))
-        elif method == "log_inter":
-            lmd = kw.get("lmd", 0.8)
-            self.sigma_hat = (1 - lmd) * torch.log1p(self.sigma_hat) + lmd * torch.ones_like(self.sigma_hat)
-        else:
-            raise ValueError(f"unknown method {method}")
-
-    def apply_sigma_hat_cpu(self, i):
-        """Every sigma_mini_batch_size steps: the accumulated spectrum becomes the
-        mass (see the module docstring for the steps)."""
+    def apply(self, i):
+        """At every ``sigma_mini_batch_size``-th step (``i > 0``) the spectrum
+        becomes the mass spectrum ``sigma_hat``."""
         if not (i % self.sigma_mini_batch_size == 0 and i > 0):
             return
-        self.sigma_hat = self.sigma_hat_cpu.to(self.sigma_hat.device)
-        flat = self.sigma_hat.view(self.sigma_hat.size(0), self.sigma_hat.size(1), -1)
-        q = torch.quantile(flat, 0.99, dim=-1, keepdim=True).view(self.sigma_hat.size(0), self.sigma_hat.size(1),
-                                                                  1, 1, 1)
-        self.stabilize_sigma_hat(method="clamp", sgm_min=0, sgm_max=q.mean())
-        lam = self.lambda_
-        self.sigma_hat = (self.sigma_hat ** lam - 1) / lam
-        mn = self.sigma_hat.amin(dim=(2, 3, 4), keepdim=True)
-        mx = self.sigma_hat.amax(dim=(2, 3, 4), keepdim=True)
-        self.sigma_hat = (self.sigma_hat - mn) / (mx - mn).clamp(min=1e-8) * (self.sig_max - self.sig_min) + self.sig_min
-        self.sigma_hat = self.sigma_hat - self.sigma_hat.mean(dim=(2, 3, 4), keepdim=True) + 1
-        self.stabilize_sigma_hat(method="shrink", lmd=self.lmd)
-        if self.mass_mode == -1:
-            self.sigma_hat = self.sigma_hat ** (-1)
+        rows = self.spectrum.reshape(self.bs * 2, -1)
+        clamp_hi = torch.quantile(rows, 0.99, dim=-1).mean().reshape(1).contiguous()
+        _lib.call(f"qedf_fm_mass_{self._sfx}", ptr(self.spectrum), ptr(self.sigma_hat), rows.shape[0], rows.shape[1],
+                  ptr(clamp_hi), float(self.lambda_), float(self.sig_min), float(self.sig_max), float(self.lmd),
+                  1 if self.mass_mode == -1 else 0, stream_handle())
 
-    def draw_momentum_fft(self, generator=None):
-        """Momenta [bs, 2, Lx, Ly, Ltau] with the Fourier mass.  The normal draws
-        are float32, as the reference's (torch's default dtype)."""
+    # the reference's names (its statistics live on the host; here on the device)
+    def update_sigma_hat_cpu(self, boson, i):
+        self.update(boson, i)
+
+    def apply_sigma_hat_cpu(self, i):
+        self.apply(i)
+
+    @property
+    def sigma_hat_cpu(self):
+        return self.spectrum.cpu()
+
+    @property
+    def boson_mean_cpu(self):
+        return self.field_mean.cpu()
+
+    # ---- momenta ------------------------------------------------------------
+    def draw_momentum_fft(self, generator=None, noise=None):
+        """Momenta ``[bs, 2, Lx, Ly, Ltau]`` with the Fourier mass.  The two
+        normal draws are float32 like the reference's (torch's default dtype);
+        ``noise = (a, b)`` supplies them instead."""
         shape = self.sigma_hat.shape
-        x = torch.randn(shape, device=self.device, dtype=torch.float32, generator=generator)
-        y = torch.randn(shape, device=self.device, dtype=torch.float32, generator=generator)
-        z = (x + 1j * y) / torch.sqrt(self.sigma_hat * self.multiplier)
-        return torch.fft.irfftn(z, (self.Lx, self.Ly, self.Ltau), norm="ortho")
+        if noise is None:
+            a = torch.randn(shape, device=self.device, dtype=torch.float32, generator=generator)
+            b = torch.randn(shape, device=self.device, dtype=torch.float32, generator=generator)
+        else:
+            a, b = noise
+        a = a.to(device=self.device, dtype=self.dtype).contiguous()
+        b = b.to(device=self.device, dtype=self.dtype).contiguous()
+        cdt = torch.complex64 if self.dtype == torch.float32 else torch.complex128
+        z = torch.empty(shape, device=self.device, dtype=cdt)
+        _lib.call(f"qedf_fm_noise_{self._sfx}", ptr(a), ptr(b), ptr(self.sigma_hat), ptr(torch.view_as_real(z)),
+                  a.numel(), self.nk, stream_handle())
+        return torch.fft.irfftn(z, self.grid, norm="ortho")
 
     def apply_m_inv(self, p):
-        """M^{-1} p = F^{-1} sigma_hat F p."""
-        pf = torch.fft.rfftn(p, (self.Lx, self.Ly, self.Ltau)) * self.sigma_hat
-        return torch.fft.irfftn(pf, (self.Lx, self.Ly, self.Ltau))
+        """``M^-1 p = F^-1 (sigma_hat F p)``."""
+        P = torch.fft.rfftn(p.to(device=self.device, dtype=self.dtype), self.grid).contiguous()
+        _lib.call(f"qedf_fm_scale_{self._sfx}", ptr(torch.view_as_real(P)), ptr(self.sigma_hat), P.numel(),
+                  stream_handle())
+        return torch.fft.irfftn(P, self.grid)

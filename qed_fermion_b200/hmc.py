@@ -212,9 +212,6 @@ class HmcSampler:
     def apply_sigma_hat_cpu(self, i):
         self.fourier_mass.apply_sigma_hat_cpu(i)
 
-    def stabilize_sigma_hat(self, method="shrink", **kw):
-        self.fourier_mass.stabilize_sigma_hat(method, **kw)
-
     def draw_momentum_fft(self):
         return self.fourier_mass.draw_momentum_fft(self.generator)
 
