@@ -106,14 +106,6 @@ int qedf_force_f_c64(const float* boson, const float* xi, float* F, int bs, int 
 int qedf_force_f_c128(const double* boson, const double* xi, double* F, int bs, int Lx, int Ltau,
                       double dtau, int rhs_per_boson, int by, int slab, qedf_stream_t stream);
 
-/* Bounded device-side waits of the operator kernels that ran out since the
- * last call: the single-precision M^dag M stages each slice of its input in
- * shared memory by a bulk copy, and a block that waits longer than about a
- * second for one gives up and counts it here (that launch's output is then
- * invalid).  Reads and clears the counter; synchronises with the device.
- * No counterpart in the reference, whose kernels are not bounded. */
-int qedf_wait_timeouts(unsigned int* count);
-
 /* ---------------------------------------------------------------------------
  * Boson part (angle layout).  K_int, J_int as HmcSampler scales them
  * (hmc_sampler_batch.py:166-175): ctau = 1 / (J_int dtau^2).
@@ -260,9 +252,10 @@ typedef struct {
                          it is (cudaLimitPersistingL2CacheSize is never changed), released
                          to normal status after the solve by one small kernel;
                          -1: no window and no extra kernel */
-  int stage;          /* 0 (default): the operator passes stage their input slices in shared
-                         memory by bulk copies where the stages fit (single-precision
-                         iterations); -1: the engine that loads them directly */
+  int stage;          /* 1: the operator passes stage their input slices in shared memory by
+                         bulk copies where the stages fit (single-precision iterations);
+                         0 (default) or -1: the engine that loads them directly.  The
+                         MIXED_BF16 mode always stages. */
 } qedf_pcg_opts;
 
 /* Bytes of device workspace qedf_pcg_solve needs for these systems. */

@@ -80,7 +80,6 @@ for _r in ("f32", "f64"):
         c_int, [_vp, _vp, c_int, c_int64, _vp, c_double, c_double, c_double, c_double, c_int, _vp])
     SIGNATURES[f"qedf_fm_noise_{_r}"] = (c_int, [_vp, _vp, _vp, _vp, c_int64, c_int, _vp])
     SIGNATURES[f"qedf_fm_scale_{_r}"] = (c_int, [_vp, _vp, c_int64, _vp])
-SIGNATURES["qedf_wait_timeouts"] = (c_int, [POINTER(ctypes.c_uint)])
 SIGNATURES["qedf_precon_tau_csr"] = (c_int, [c_int, POINTER(c_int), POINTER(c_int), POINTER(c_double),
                                               POINTER(c_int)])
 SIGNATURES["qedf_pcg_workspace_bytes"] = (c_int64, [POINTER(QedfSystem), c_int, POINTER(QedfPcgOpts)])
@@ -95,8 +94,7 @@ _LIB = None
 # kernel launches issued through ``call`` (compute entry points launch one
 # kernel each; qedf_pcg_solve launches one persistent kernel)
 LAUNCHES = {"count": 0}
-_HOST_ONLY = {"qedf_version", "qedf_status_string", "qedf_precon_tau_csr", "qedf_pcg_workspace_bytes",
-              "qedf_wait_timeouts"}
+_HOST_ONLY = {"qedf_version", "qedf_status_string", "qedf_precon_tau_csr", "qedf_pcg_workspace_bytes"}
 
 
 class QedfError(RuntimeError):
@@ -139,13 +137,6 @@ def call(name, *args):
     if st != QEDF_OK:
         raise QedfError(name, st, lib.qedf_status_string(st).decode())
     return st
-
-
-def wait_timeouts():
-    """Operator-kernel waits that gave up since the last call (then cleared)."""
-    n = ctypes.c_uint(0)
-    call("qedf_wait_timeouts", ctypes.byref(n))
-    return int(n.value)
 
 
 def status_string(st):

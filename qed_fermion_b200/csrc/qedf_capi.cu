@@ -39,8 +39,6 @@ int op_entry(int op, const A* boson, const R* x, R* out, int bs, int Lx, int Lta
   a.rhs_per_phi = rhs_per_boson;
   a.T = slab;
   a.xs = 1;
-  a.stage = 1;
-  a.stage_off = 0;
   a.c1 = f.c1;
   a.ch = f.ch;
   a.t1 = f.t1;
@@ -308,11 +306,6 @@ int qedf_cdot_c64(const float* u, const float* v, int64_t n, int rows, double* o
 int qedf_cdot_c128(const double* u, const double* v, int64_t n, int rows, double* out, qedf_stream_t s) {
   if (!u || !v || !out || n < 1 || rows < 1 || rows > 65535) return QEDF_ERR_ARG;
   return launch_cdot<double>(u, v, n, rows, out, reinterpret_cast<cudaStream_t>(s));
-}
-
-int qedf_wait_timeouts(unsigned int* count) {
-  if (!count) return QEDF_ERR_ARG;
-  return read_wait_timeouts(count);
 }
 
 int64_t qedf_pcg_workspace_bytes(const qedf_system* sys, int nsys, const qedf_pcg_opts* opts) {

@@ -18,8 +18,6 @@ struct OpArgs {
   int rhs_per_phi;  // consecutive vectors sharing one angle array
   int T;            // slab length (0 = auto)
   int xs;           // allow the warp-shuffle engine (single precision, L <= 64)
-  int stage;        // allow the staged M^dag M engine (single precision)
-  int stage_off;    // bytes: start of the slice stages in dynamic shared memory
   double c1, ch, t1, th, Cb;
 };
 
@@ -66,8 +64,7 @@ struct KickArgs {
 };
 
 int num_sms();
-// count of operator-kernel waits that gave up since the last read (then cleared)
-int read_wait_timeouts(unsigned int* count);
+
 // tile height (rows of the 2 x by site block per thread) for an L x L slice;
 // requested = 0 picks automatically; -1 if no valid tile exists
 int pick_by(int L, int requested, int real_bytes);

@@ -25,23 +25,13 @@ namespace qedf {
 //   (M^dag M x)_t: y = M x is produced slice by slice in registers and M^dag
 //                  applied to it, so x is read once and one extra slice of y
 //                  (the slab's lower halo) is recomputed.
-// Bounded waits of the operator kernels that ran out (a bulk copy that did not
-// arrive within the budget); qedf_wait_timeouts reads and clears the count.
-__device__ unsigned int g_wait_timeouts;
-
-// SM cycles a block waits for a staged slice before it gives up (~1 s)
-constexpr long long OP_STAGE_BUDGET = 2000000000ll;
-
 template <typename R, typename A, int BY, int OP, int EC>
 __global__ void __launch_bounds__(MaxT<BY, EC>::value, MaxT<BY, EC>::min_blocks) k_operator(OpArgs p) {
-  extern __shared__ __align__(128) unsigned char smem[];
+  extern __shared__ __align__(16) unsigned char smem[];
   constexpr bool PHS = (EC & EC_PHS) != 0;
   constexpr bool STASH = (EC & EC_NOSTASH) == 0;
   constexpr bool XS = (EC & EC_XS) != 0;
-  constexpr bool STG = (EC & EC_STAGE) != 0;
-  static_assert(!STG || (STASH && !XS), "the staged engine keeps y_t in the stash");
   constexpr int LT = ec_fixed_l(EC);
-  __shared__ unsigned long long stg_bar[2];
   Slice<R, BY, PHS, XS, LT> S;
   const int L = lattice_l<EC>(p.L);
   S.init(L, smem, 2, (R)p.c1, (R)p.ch, threadIdx.x);
@@ -60,7 +50,6 @@ __global__ void __launch_bounds__(MaxT<BY, EC>::value, MaxT<BY, EC>::min_blocks)
   Cx<R> X0[BY][2], X1[BY][2], Y[BY][2];
   Cx<R> Yp[STASH ? 1 : BY][2];
 
-  static_assert(!STG || OP == OP_MHM, "the staged engine is compiled for M^dag M");
   if (OP == OP_M) {
     int tp = (a - 1 + Nt) % Nt;
     if (S.on) S.load(X0, x + tp * sv);
@@ -85,59 +74,6 @@ __global__ void __launch_bounds__(MaxT<BY, EC>::value, MaxT<BY, EC>::min_blocks)
       S.template applyB<FAC_TILDE>(Y);
       if (S.on) {
         axpy_blk<R, BY>(Y, X0, sigma_of<R>(t, Nt) * Cb, Y);
-        S.store(z + t * sv, Y);
-      }
-      copy_blk<R, BY>(X0, X1);
-    }
-  } else if (STG) {  // OP_MHM, the slices of x staged whole in shared memory
-    // stage j holds slice tp + j of the sequence tp, a, ..., b (bulk copies
-    // issued by thread 0 one slice ahead); the loop is that of OP_MHM below
-    SliceStages<1> stg;
-    SliceStages<1>::init_barriers(stg_bar);
-    stg.setup(stg_bar, smem + p.stage_off, (unsigned)(Vs * sizeof(Cx<R>)));
-    const int tp = (a - 1 + Nt) % Nt;
-    const int nT = b - a;
-    auto issue = [&](int j) {
-      if (threadIdx.x != 0 || j > nT + 1) return;
-      int t = tp + j;
-      if (t >= Nt) t -= Nt;
-      const void* src[1] = {x + t * sv};
-      stg.issue(j, src, 1u);
-    };
-    auto take = [&](Cx<R> (&X)[BY][2], int j) {
-      if (!stg.wait(j, OP_STAGE_BUDGET) && threadIdx.x == 0) atomicAdd(&g_wait_timeouts, 1u);
-      if (S.on) S.load_coherent(X, reinterpret_cast<const R*>(stg.slot(j, 0)));
-    };
-    issue(0);
-    issue(1);
-    take(X0, 0);
-    take(X1, 1);
-    A ang[BY][4];
-    if constexpr (!PHS) S.load_angles(ang, phi + a * sv);
-    S.phases(phi + tp * sv, t1, th);  // block barrier: stage 0 is read
-    issue(2);
-    S.template applyB<FAC_TILDE>(X0);
-    axpy_blk<R, BY>(Y, X1, sigma_of<R>(tp, Nt) * Cb, X0);
-    S.park(Y);
-    copy_blk<R, BY>(X0, X1);
-    for (int i = 0; i < nT; ++i) {
-      const int t = a + i;
-      issue(i + 3);  // into the buffer of stage i + 1, read before the last barriers
-      take(X1, i + 2);
-      if constexpr (!PHS) {
-        S.phases_from(ang, t1, th);
-        if (t + 1 < b) S.load_angles(ang, phi + (t + 1) * sv);
-      } else {
-        S.phases(phi + t * sv, t1, th);
-      }
-      const R sg = sigma_of<R>(t, Nt) * Cb;
-      S.template applyB<FAC_TILDE>(X0);
-      axpy_blk<R, BY>(Y, X1, sg, X0);
-      S.unpark(X0);
-      S.park(Y);
-      S.template applyB<FAC_TILDE, 1>(Y);
-      if (S.on) {
-        axpy_blk<R, BY>(Y, X0, sg, Y);
         S.store(z + t * sv, Y);
       }
       copy_blk<R, BY>(X0, X1);
@@ -863,29 +799,13 @@ int pick_by(int L, int requested, int real_bytes) {
 
 static size_t smem_limit() { return 227 * 1024; }
 
-// shared memory of the staged M^dag M: the engine's tables, then two slices of x
-template <typename R, int EC>
-static size_t stage_off_bytes(int L, int BY) { return (slice_smem_bytes<R, EC>(L, BY, 2) + 127) / 128 * 128; }
-template <typename R, int EC>
-static size_t staged_smem_bytes(int L, int BY) {
-  return stage_off_bytes<R, EC>(L, BY) + 2 * (size_t)L * L * sizeof(Cx<R>);
-}
-
 template <typename R, typename A, int BY, int EC>
-static int launch_operator_t(int op, OpArgs a, cudaStream_t st) {
+static int launch_operator_t(int op, const OpArgs& a, cudaStream_t st) {
   const int threads = slice_threads(a.L, BY, (EC & EC_XS) != 0);
-  size_t smem = slice_smem_bytes<R, EC>(a.L, BY, 2);
-  if constexpr ((EC & EC_STAGE) != 0) {
-    if (op != OP_MHM) return QEDF_ERR_ARG;
-    a.stage_off = (int)stage_off_bytes<R, EC>(a.L, BY);
-    smem = staged_smem_bytes<R, EC>(a.L, BY);
-  }
+  const size_t smem = slice_smem_bytes<R, EC>(a.L, BY, 2);
   if (smem > smem_limit() || threads > MaxT<BY, EC>::value) return QEDF_ERR_SIZE;
   dim3 grid((a.Nt + a.T - 1) / a.T, a.bs);
-  if constexpr ((EC & EC_STAGE) != 0) {
-    if (prepare_smem(k_operator<R, A, BY, OP_MHM, EC>, smem)) return QEDF_ERR_CUDA;
-    k_operator<R, A, BY, OP_MHM, EC><<<grid, threads, smem, st>>>(a);
-  } else if (op == OP_M) {
+  if (op == OP_M) {
     if (prepare_smem(k_operator<R, A, BY, OP_M, EC>, smem)) return QEDF_ERR_CUDA;
     k_operator<R, A, BY, OP_M, EC><<<grid, threads, smem, st>>>(a);
   } else if (op == OP_MH) {
@@ -902,7 +822,7 @@ static int launch_operator_t(int op, OpArgs a, cudaStream_t st) {
 // L = 48); every other L runs the run-time-L engine.
 template <typename R, typename A, int BY, int EC>
 static int launch_operator_fl(int op, const OpArgs& a, cudaStream_t st) {
-  if constexpr (EC == 0 || EC == EC_PHS || EC == EC_STAGE)
+  if constexpr (EC == 0 || EC == EC_PHS)
     return with_fixed_l<BY>(a.L, [&](auto lt) {
       return launch_operator_t<R, A, BY, EC | EC_L(decltype(lt)::value)>(op, a, st);
     });
@@ -913,9 +833,6 @@ static int launch_operator_fl(int op, const OpArgs& a, cudaStream_t st) {
 // room for the stash, y stays in registers
 template <typename R, typename A, int BY>
 static int launch_operator_by(int op, const OpArgs& a, int xs, cudaStream_t st) {
-  // single-precision M^dag M: x staged by bulk copies where the stages fit
-  if (sizeof(R) == 4 && op == OP_MHM && a.stage && staged_smem_bytes<R, 0>(a.L, BY) <= smem_limit())
-    return launch_operator_fl<R, A, BY, EC_STAGE>(op, a, st);
   if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
     return launch_operator_fl<R, A, BY, EC_PHS>(op, a, st);
   if (sizeof(R) == 4 && xs && xs_possible(a.L) && ((a.L / 2) & (a.L / 2 - 1)) == 0 &&
@@ -943,15 +860,6 @@ int launch_operator(int op, OpArgs a, int by, cudaStream_t st) {
   }
   return QEDF_ERR_ARG;
 }
-int read_wait_timeouts(unsigned int* count) {
-  unsigned int v = 0;
-  if (cudaMemcpyFromSymbol(&v, g_wait_timeouts, sizeof(v)) != cudaSuccess) return QEDF_ERR_CUDA;
-  const unsigned int zero = 0;
-  if (cudaMemcpyToSymbol(g_wait_timeouts, &zero, sizeof(zero)) != cudaSuccess) return QEDF_ERR_CUDA;
-  *count = v;
-  return QEDF_OK;
-}
-
 template int launch_operator<float, float>(int, OpArgs, int, cudaStream_t);
 template int launch_operator<double, double>(int, OpArgs, int, cudaStream_t);
 

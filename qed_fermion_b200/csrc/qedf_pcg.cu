@@ -1018,7 +1018,7 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
   p.mode = o->mode;
   p.nsys = nsys;
   p.xs = 1;
-  p.stage = o->stage < 0 ? 0 : 1;
+  p.stage = o->stage > 0 ? 1 : 0;
   p.l2 = o->l2_persist < 0 ? -1 : 0;
   if (o->chunk != 0 && o->chunk != PCG_CHUNK) return QEDF_ERR_ARG;
   p.CH = PCG_CHUNK;

@@ -72,17 +72,18 @@ class PcgSolver:
     (:mod:`qed_fermion_b200.autotune`), which times the candidates once per
     problem shape and caches the winner; explicit ``by`` / ``slab`` win over it.
 
-    ``stage`` (default on) lets the single-precision operator passes stage
-    their input slices in shared memory by bulk copies where the stages fit;
-    False selects the engine that loads them directly (the results are the
-    same bit for bit).
+    ``stage`` lets the single-precision operator passes stage their input
+    slices in shared memory by bulk copies where the stages fit (the results
+    are the same bit for bit; measured no faster on the benchmark lattice, so
+    off by default and left to the autotuner).  The "mixed_bf16" mode always
+    stages.
     """
 
     def __init__(self, systems: Sequence[System], mode: str = "mixed", rtol: float = 1e-10,
                  max_iter: int = 10000, dtau: float = 0.1, use_precon: bool = True,
                  ru_interval: int = 50, ru_delta: float = 0.1, by: int = 0, slab: int = 0,
                  chunk: int = 0, timeout_ms: float = 2000.0, profile: bool = False, device=None,
-                 l2_persist: bool = True, stage: bool = True, tune: bool = False):
+                 l2_persist: bool = True, stage: bool = False, tune: bool = False):
         if mode not in MODES:
             raise ValueError(f"mode must be one of {sorted(MODES)}")
         self.systems = [s if isinstance(s, System) else System(*s) for s in systems]
@@ -104,7 +105,7 @@ class PcgSolver:
                                       1 if use_precon else 0, int(ru_interval), float(ru_delta), int(by),
                                       int(slab), int(chunk), float(timeout_ms),
                                       self.profile.data_ptr() if profile else None,
-                                      0 if l2_persist else -1, 0 if stage else -1)
+                                      0 if l2_persist else -1, 1 if stage else 0)
         nbytes = _lib.load().qedf_pcg_workspace_bytes(self._sys, n, self._opts)
         if nbytes < 0:
             raise ValueError("invalid system description for the PCG solver")
