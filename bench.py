@@ -510,8 +510,9 @@ def run_native(args):
         hb16 = make("mixed_bf16")
         hb16.boson = hmc.boson.clone()
         bf16 = time_trajectories(hb16, args.bf16_steps)
-        bf16["path"] = "mixed precision with the PCG's vectors stored as bf16 pairs"
-        bf16["pcg_bytes_per_site_iteration"] = 7 * 4 + 2 * 4
+        bf16["path"] = "mixed precision with the PCG's p and z stored as bf16 pairs"
+        # read p (bf16), x, r, angles; write x, r, p (bf16)
+        bf16["pcg_bytes_per_site_iteration"] = 2 * 4 + 4 * 8 + 2 * 4
         del hb16
 
     # --- Delta H of one shared trajectory: mixed and bf16 storage against FP64
@@ -669,7 +670,7 @@ def run_solve_only(args):
     it = int(res.iters.max())
     n = L * L * Lt * bs
     # bytes per site and iteration: 7 vector accesses and the two angles
-    bps = {"mixed": 64, "fp32": 64, "fp64": 128, "mixed_bf16": 36}[args.mode]
+    bps = {"mixed": 64, "fp32": 64, "fp64": 128, "mixed_bf16": 48}[args.mode]
     print(json.dumps({"solve_only": True, "mode": args.mode, "lattice": [L, L, Lt], "rhs": bs, "iters": it,
                       "ms": ms, "us_per_iter": ms * 1e3 / max(it, 1), "bytes_per_site_iter": bps,
                       "algorithmic_GBps": n * bps * it / (ms / 1e3) / 1e9}), flush=True)

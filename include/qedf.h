@@ -228,10 +228,11 @@ typedef struct {
 #define QEDF_PCG_PLAIN_F64 1 /* complex128 vectors, double angles, double arithmetic */
 #define QEDF_PCG_MIXED 2     /* complex128 b/x, float angles; float iterations with
                                 double reliable updates of x and the true residual */
-#define QEDF_PCG_MIXED_BF16 3 /* as QEDF_PCG_MIXED, with the iteration vectors (r, p, z,
-                                 M^dag M p, the float part of x) stored as bf16 pairs:
-                                 4 bytes per complex number, float arithmetic; lattices
-                                 whose slice stages fit in shared memory (L <= 66) */
+#define QEDF_PCG_MIXED_BF16 3 /* as QEDF_PCG_MIXED, with the search direction p and the
+                                 preconditioned residual z stored as bf16 pairs (4 bytes
+                                 per complex number); r, M^dag M p and the float part of x
+                                 stay float, as does the arithmetic; lattices whose slice
+                                 stages fit in shared memory */
 
 typedef struct {
   int mode;           /* QEDF_PCG_* */

@@ -119,7 +119,8 @@ __device__ __forceinline__ void st2(double* p, Cx<double> a, Cx<double> b) {
   reinterpret_cast<double2*>(p)[1] = make_double2(b.re, b.im);
 }
 // Storage of single-precision iteration vectors: float (complex64) or bf16
-// pairs (4 bytes per complex number, the BF16 storage option of the PCG).
+// pairs (4 bytes per complex number, the PCG's BF16 storage option for its
+// search direction and preconditioned residual).
 // ld2s / st2s move two consecutive complex numbers (16 B as float, 8 B as
 // bf16); arithmetic stays in float.  round_st returns the value the storage
 // keeps (round to nearest even for bf16), so that values kept in registers
@@ -143,11 +144,6 @@ __device__ __forceinline__ void st2s(bf16* p, Cx<float> a, Cx<float> b) {
   q.x = *reinterpret_cast<const unsigned*>(&lo);
   q.y = *reinterpret_cast<const unsigned*>(&hi);
   *reinterpret_cast<uint2*>(p) = q;
-}
-template <typename S>
-__device__ __forceinline__ S to_st(double v) {
-  if constexpr (std::is_same<S, bf16>::value) return __float2bfloat16_rn((float)v);
-  else return (S)v;
 }
 template <typename S, typename R>
 __device__ __forceinline__ Cx<R> round_st(Cx<R> v) {
@@ -183,12 +179,6 @@ __device__ __forceinline__ void st4(double* p, const double (&a)[4]) {
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
-}
-// 8-byte variant (bf16 pairs of two sites); it allocates in L1 like a plain
-// load, which the grid barrier's acquire makes coherent in the same way
-__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -244,13 +234,15 @@ template <int NARR>
 struct SliceStages {
   unsigned long long* bar;  // [2], static shared memory, initialised once per kernel
   unsigned char* buf;       // [2][NARR][bytes]
-  unsigned bytes;           // bytes of one slice array
+  unsigned bytes;           // slot stride: bytes of the widest slice array
+  unsigned sizes[NARR];     // bytes copied into slot k (at most `bytes`)
   unsigned uses[2];
 
   __device__ void setup(unsigned long long* bars, unsigned char* buffers, unsigned slice_bytes) {
     bar = bars;
     buf = buffers;
     bytes = slice_bytes;
+    for (int k = 0; k < NARR; ++k) sizes[k] = slice_bytes;
     uses[0] = uses[1] = 0;
   }
   // once per kernel, by every thread (contains a block barrier)
@@ -269,12 +261,13 @@ struct SliceStages {
   __device__ void issue(int j, const void* const (&src)[NARR], unsigned mask) {
     unsigned n = 0;
 #pragma unroll
-    for (int k = 0; k < NARR; ++k) n += (mask >> k) & 1u;
+    for (int k = 0; k < NARR; ++k)
+      if ((mask >> k) & 1u) n += sizes[k];
     fence_proxy_async_global();
-    mbar_arrive_expect_tx(bar + (j & 1), n * bytes);
+    mbar_arrive_expect_tx(bar + (j & 1), n);
 #pragma unroll
     for (int k = 0; k < NARR; ++k)
-      if ((mask >> k) & 1u) bulk_copy_g2s(slot(j, k), src[k], bytes, bar + (j & 1));
+      if ((mask >> k) & 1u) bulk_copy_g2s(slot(j, k), src[k], sizes[k], bar + (j & 1));
   }
   // every thread: wait for stage j; false if the bounded wait gave up
   __device__ bool wait(int j, long long budget) {

@@ -218,10 +218,12 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   constexpr bool PHS_H = (ECH & EC_PHS) != 0, STASH_H = (ECH & EC_NOSTASH) == 0;
   constexpr bool STG_S = (ECS & EC_STAGE) != 0;
   static_assert(!STG_S || (STASH_S && !XS_S), "the staged engine keeps y_t in the stash");
-  // storage of the iteration vectors r, p, z, M^dag M p and x_lo: the
-  // iteration precision, or bf16 pairs (EC_BF16, staged engine, mixed mode)
+  // storage of the search direction p and the preconditioned residual z: the
+  // iteration precision, or bf16 pairs (EC_BF16, staged engine, mixed mode).
+  // r, M^dag M p and x_lo always keep the iteration precision, so that the
+  // residual recurrence r -= alpha M^dag M p stays that of x += alpha p.
   constexpr bool BF = (ECS & EC_BF16) != 0;
-  using ST = typename std::conditional<BF, bf16, RS>::type;
+  using SP = typename std::conditional<BF, bf16, RS>::type;
   static_assert(!BF || (STG_S && sizeof(RS) == 4 && !std::is_same<RS, RH>::value),
                 "bf16 storage is a mixed-precision mode of the staged engine");
   extern __shared__ __align__(128) unsigned char dsm[];
@@ -235,11 +237,11 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   Acc acc(p.acc, NV);
   const unsigned int nblk = gridDim.x;
   const int tid = threadIdx.x;
-  const ST* zbuf = reinterpret_cast<const ST*>(p.z);
-  ST* r = reinterpret_cast<ST*>(p.r);
-  ST* z = reinterpret_cast<ST*>(p.z);
-  ST* Op = reinterpret_cast<ST*>(p.Op);
-  ST* xs = MIXED ? reinterpret_cast<ST*>(p.xlo) : reinterpret_cast<ST*>(p.x);
+  const SP* zbuf = reinterpret_cast<const SP*>(p.z);
+  RS* r = reinterpret_cast<RS*>(p.r);
+  SP* z = reinterpret_cast<SP*>(p.z);
+  RS* Op = reinterpret_cast<RS*>(p.Op);
+  RS* xs = MIXED ? reinterpret_cast<RS*>(p.xlo) : reinterpret_cast<RS*>(p.x);
   RH* xh = reinterpret_cast<RH*>(p.x);
   const RH* bvec = reinterpret_cast<const RH*>(p.b);
   const A* phi_all = reinterpret_cast<const A*>(p.phi);
@@ -297,7 +299,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const int64_t base = vec_base(s, v);
     Cx<RS>* rsm = reinterpret_cast<Cx<RS>*>(dsm);
     const RS al = (RS)st.alpha[v];
-    const ST* opv = Op;
+    const RS* opv = Op;
     const int j = tid % PPR;
     const int rstep = blockDim.x / PPR;
     const bool jon = 2 * j < w;
@@ -318,13 +320,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         if (k < K) {
           const int64_t i2 = 2 * (base + (int64_t)(t0 + k * rstep) * Vs + c0 + 2 * j);
           uint4* d = stg + (size_t)(k % PCG_EW_STAGES) * 2 * nthr + tid;
-          if constexpr (sizeof(ST) == 4) {
-            cp_async16(d, opv + i2);
-            cp_async16(d + nthr, r + i2);
-          } else {  // bf16 pairs: 8 bytes a vector
-            cp_async8(d, opv + i2);
-            cp_async8(d + nthr, r + i2);
-          }
+          cp_async16(d, opv + i2);
+          cp_async16(d + nthr, r + i2);
         }
         cp_async_commit();
       };
@@ -334,10 +331,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         cp_async_wait<PCG_EW_STAGES - 1>();
         const uint4* d = stg + (size_t)(k % PCG_EW_STAGES) * 2 * nthr + tid;
         Cx<RS> o0, o1, r0, r1;
-        ld2s(reinterpret_cast<const ST*>(d), o0, o1);
-        ld2s(reinterpret_cast<const ST*>(d + nthr), r0, r1);
-        r0 = round_st<ST>(mk<RS>(fma(-al, o0.re, r0.re), fma(-al, o0.im, r0.im)));
-        r1 = round_st<ST>(mk<RS>(fma(-al, o1.re, r1.re), fma(-al, o1.im, r1.im)));
+        ld2c(reinterpret_cast<const RS*>(d), o0, o1);
+        ld2c(reinterpret_cast<const RS*>(d + nthr), r0, r1);
+        r0 = mk<RS>(fma(-al, o0.re, r0.re), fma(-al, o0.im, r0.im));
+        r1 = mk<RS>(fma(-al, o1.re, r1.re), fma(-al, o1.im, r1.im));
         const int t = t0 + k * rstep;
         const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
         st2s(r + i2, r0, r1);
@@ -357,8 +354,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         Cx<RH> b0, b1;
         ld2c(bvec + i2, b0, b1);
         acc_a += (double)b0.re * b0.re + (double)b0.im * b0.im + (double)b1.re * b1.re + (double)b1.im * b1.im;
-        r0 = round_st<ST>(mk<RS>((RS)b0.re, (RS)b0.im));
-        r1 = round_st<ST>(mk<RS>((RS)b1.re, (RS)b1.im));
+        r0 = mk<RS>((RS)b0.re, (RS)b0.im);
+        r1 = mk<RS>((RS)b1.re, (RS)b1.im);
         st2s(xs + i2, mk<RS>(0, 0), mk<RS>(0, 0));
         if (MIXED) st2(xh + i2, mk<RH>(0, 0), mk<RH>(0, 0));
         st2s(r + i2, r0, r1);
@@ -366,8 +363,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         Cx<RS> o0, o1;
         ld2s(opv + i2, o0, o1);
         ld2s(r + i2, r0, r1);
-        r0 = round_st<ST>(mk<RS>(fma(-al, o0.re, r0.re), fma(-al, o0.im, r0.im)));
-        r1 = round_st<ST>(mk<RS>(fma(-al, o1.re, r1.re), fma(-al, o1.im, r1.im)));
+        r0 = mk<RS>(fma(-al, o0.re, r0.re), fma(-al, o0.im, r0.im));
+        r1 = mk<RS>(fma(-al, o1.re, r1.re), fma(-al, o1.im, r1.im));
         st2s(r + i2, r0, r1);
       } else {
         ld2s(r + i2, r0, r1);
@@ -413,8 +410,14 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
           }
         }
         const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
-        z0 = round_st<ST>(z0);
-        z1 = round_st<ST>(z1);
+        z0 = round_st<SP>(z0);
+        z1 = round_st<SP>(z1);
+        st2s(z + i2, z0, z1);
+      } else if (BF) {
+        // the bf16 engine reads z even without a preconditioner: z = r, rounded
+        const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
+        z0 = round_st<SP>(z0);
+        z1 = round_st<SP>(z1);
         st2s(z + i2, z0, z1);
       }
       bpart = fma(r0.re, z0.re, fma(r0.im, z0.im, fma(r1.re, z1.re, fma(r1.im, z1.im, bpart))));
@@ -570,13 +573,16 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const bool has_old = st.iters[v] > 0;
     const bool pend = st.pending[v];
     const RS al_old = (RS)st.alpha[v];
-    ST* xl = xs + vb;
-    const ST* pold = reinterpret_cast<const ST*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
-    ST* pnew = reinterpret_cast<ST*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
-    const ST* zz = (S.precon ? zbuf : reinterpret_cast<const ST*>(r)) + vb;
-    ST* O = Op + vb;
+    RS* xl = xs + vb;
+    const SP* pold = reinterpret_cast<const SP*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
+    SP* pnew = reinterpret_cast<SP*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
+    const SP* zz = ((S.precon || BF) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
+    RS* O = Op + vb;
     const RS t1 = (RS)p.t1, th = (RS)p.th, Cb = (RS)p.Cb;
-    stg.bytes = (unsigned)(Vs * 2 * sizeof(ST));
+    // slots of the iteration precision; z and p_old may be narrower
+    stg.bytes = (unsigned)(Vs * 2 * sizeof(RS));
+    stg.sizes[0] = stg.sizes[1] = (unsigned)(Vs * 2 * sizeof(SP));
+    stg.sizes[2] = stg.bytes;
     const int nT = bnd - a;  // own slices
     const int tp = (a - 1 + Nt) % Nt;
     auto slice_of = [&](int j) { const int t = tp + j; return t >= Nt ? t - Nt : t; };
@@ -594,13 +600,13 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     // also x_lo += alpha_old p_old
     auto getp = [&](Cx<RS> (&X)[BY][2], int j, bool own) {
       if (!E.on) return;
-      E.load_st(X, reinterpret_cast<const ST*>(stg.slot(j, 0)));
+      E.load_st(X, reinterpret_cast<const SP*>(stg.slot(j, 0)));
       if (has_old) {
         Cx<RS> T0[BY][2];
-        E.load_st(T0, reinterpret_cast<const ST*>(stg.slot(j, 1)));
+        E.load_st(T0, reinterpret_cast<const SP*>(stg.slot(j, 1)));
         if (own && pend) {
           Cx<RS> XL[BY][2];
-          E.load_st(XL, reinterpret_cast<const ST*>(stg.slot(j, 2)));
+          E.load_coherent(XL, reinterpret_cast<const RS*>(stg.slot(j, 2)));
 #pragma unroll
           for (int q = 0; q < BY; ++q)
 #pragma unroll
@@ -608,7 +614,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
               XL[q][c].re = fma(al_old, T0[q][c].re, XL[q][c].re);
               XL[q][c].im = fma(al_old, T0[q][c].im, XL[q][c].im);
             }
-          E.store_st(xl + slice_of(j) * sv, XL);
+          E.store(xl + slice_of(j) * sv, XL);
         }
 #pragma unroll
         for (int q = 0; q < BY; ++q)
@@ -616,7 +622,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
           for (int c = 0; c < 2; ++c) {
             X[q][c].re = fma(beta, T0[q][c].re, X[q][c].re);
             X[q][c].im = fma(beta, T0[q][c].im, X[q][c].im);
-            X[q][c] = round_st<ST>(X[q][c]);
+            X[q][c] = round_st<SP>(X[q][c]);
           }
       }
     };
@@ -665,7 +671,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       E.template applyB<FAC_TILDE, 1>(Y);     // B_t y_{t+1}
       if (E.on) {
         axpy_blk<RS, BY>(Y, X0, sg, Y);        // (M^dag M p)_t
-        E.store_st(O + t * sv, Y);
+        E.store(O + t * sv, Y);
       }
       copy_blk<RS, BY>(X0, X1);
     }
@@ -691,7 +697,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const A* phi = phi_all + S.phi0 + (S.shared ? 0 : (int64_t)(v - S.rhs0) * Nt * sv);
     const RH* xx = xh + vb;
     const RH* bb = bvec + vb;
-    ST* rout = r + vb;
+    RS* rout = r + vb;
     const RH t1 = (RH)p.t1, th = (RH)p.th, Cb = (RH)p.Cb;
     Cx<RH> X0[BY][2], X1[BY][2], Y[BY][2];
     Cx<RH> Yp[STASH_H ? 1 : BY][2];
@@ -731,8 +737,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
             const RH dr = X0[q][c].re - Y[q][c].re, di = X0[q][c].im - Y[q][c].im;
             rr_acc += (double)dr * dr + (double)di * di;
             const int64_t site = (int64_t)t * Vs + (E.y0 + q) * SL(S) + E.x0 + c;
-            rout[2 * site] = to_st<ST>(dr);
-            rout[2 * site + 1] = to_st<ST>(di);
+            rout[2 * site] = (RS)dr;
+            rout[2 * site + 1] = (RS)di;
           }
       }
       copy_blk<RH, BY>(X0, X1);
@@ -745,7 +751,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   // the pending x += alpha p_last of right-hand side v at one site pair
   auto apply_pending = [&](int v, int64_t i2, Cx<RS>& l0, Cx<RS>& l1) {
     if (!st.pending[v]) return;
-    const ST* pl = reinterpret_cast<const ST*>((st.iters[v] & 1) ? p.p0 : p.p1);  // p of the last iteration
+    const SP* pl = reinterpret_cast<const SP*>((st.iters[v] & 1) ? p.p0 : p.p1);  // p of the last iteration
     const RS al = (RS)st.alpha[v];
     Cx<RS> p0v, p1v;
     ld2s(pl + i2, p0v, p1v);
@@ -980,13 +986,13 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
 // ---------------------------------------------------------------------------
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // shared memory of the operator passes' slice stages: 2 buffers x 3 slices of
-// the storage type ST
-template <typename ST>
-static size_t pcg_stage_bytes(int L) { return 2 * 3 * (size_t)L * L * 2 * sizeof(ST); }
+// the iteration precision RS
+template <typename RS>
+static size_t pcg_stage_bytes(int L) { return 2 * 3 * (size_t)L * L * 2 * sizeof(RS); }
 
-int pcg_storage_bytes(int mode) {
-  return mode == QEDF_PCG_PLAIN_F64 ? 8 : (mode == QEDF_PCG_MIXED_BF16 ? 2 : 4);
-}
+// (MIXED_BF16 keeps r, M^dag M p and x_lo in float; its p and z buffers use
+// half of their float-sized room)
+int pcg_storage_bytes(int mode) { return mode == QEDF_PCG_PLAIN_F64 ? 8 : 4; }
 
 // Slab length of the operator units: units are dealt to the blocks in turn,
 // so the busiest block runs ceil(units / nblk) units of T slices plus one
@@ -1224,7 +1230,7 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   size_t smem = slice_smem_bytes<RS, ECS>(Lmax, BY, 2);
   if (ECS & EC_STAGE) {
     p.stage_off = (int)align_up(smem, 128);
-    smem = p.stage_off + ((ECS & EC_BF16) ? pcg_stage_bytes<bf16>(Lmax) : pcg_stage_bytes<RS>(Lmax));
+    smem = p.stage_off + pcg_stage_bytes<RS>(Lmax);
   }
   smem = std::max(smem, slice_smem_bytes<RH, ECH>(Lmax, BY, 2));
   // elementwise units: the r column, and in single precision the staging
@@ -1281,10 +1287,10 @@ int launch_pcg_prep(const PcgParams& p, int zero_words, cudaStream_t st) {
 }
 
 static bool fits(size_t engine_bytes) { return engine_bytes + sizeof(RhsState) <= 227 * 1024; }
-// the staged engine: its tables plus two stages of three slices of ST
-template <typename RS, int ECS, typename ST = RS>
+// the staged engine: its tables plus two stages of three slices
+template <typename RS, int ECS>
 static bool fits_staged(int L, int BY) {
-  return align_up(slice_smem_bytes<RS, ECS>(L, BY, 2), 128) + pcg_stage_bytes<ST>(L) + sizeof(RhsState) <=
+  return align_up(slice_smem_bytes<RS, ECS>(L, BY, 2), 128) + pcg_stage_bytes<RS>(L) + sizeof(RhsState) <=
          227 * 1024;
 }
 
@@ -1336,9 +1342,9 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
       return launch_pcg_t<float, double, float, BY, 0, EC_NOSTASH>(p, st);
     case QEDF_PCG_MIXED_BF16:
       // bf16 storage exists for the staged engine only
-      if (fits_staged<float, 0, bf16>(Lmax, BY) && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
+      if (fits_staged<float, 0>(Lmax, BY) && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
         return launch_pcg_fl<float, double, float, BY, EC_STAGE | EC_BF16, EC_PHS>(p, st);
-      if (fits_staged<float, 0, bf16>(Lmax, BY) && fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
+      if (fits_staged<float, 0>(Lmax, BY) && fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
         return launch_pcg_fl<float, double, float, BY, EC_STAGE | EC_BF16, 0>(p, st);
       return QEDF_ERR_SIZE;
   }

@@ -12,10 +12,11 @@ Precision modes:
   "mixed" complex128 b and x, float32 angles, float iterations with double
           reliable updates (x accumulated and the true residual recomputed in
           double), so the solution meets rtol down to ~1e-12;
-  "mixed_bf16" the same with the iteration vectors (r, p, z, M^dag M p and
-          the float part of x) stored as bf16 pairs, 4 bytes per complex
-          number; the arithmetic stays in float and convergence is still
-          decided on the double-precision true residual.
+  "mixed_bf16" the same with the search direction p and the preconditioned
+          residual z stored as bf16 pairs, 4 bytes per complex number; r,
+          M^dag M p and the float part of x stay float, so the residual
+          recurrence matches the x updates; convergence is still decided on
+          the double-precision true residual.
 """
 from __future__ import annotations
 
