@@ -34,10 +34,7 @@ __global__ void __launch_bounds__(MaxT<BY, EC>::value, MaxT<BY, EC>::min_blocks)
   constexpr int LT = ec_fixed_l(EC);
   Slice<R, BY, PHS, XS, LT> S;
   const int L = lattice_l<EC>(p.L);
-  constexpr bool PAIR = (EC & EC_PAIR) != 0;
-  static_assert(!PAIR || (PHS && !XS && STASH), "the paired engine keeps its phases in shared memory");
-  S.init(L, smem, PAIR ? 4 : 2, (R)p.c1, (R)p.ch, threadIdx.x);
-  if (PAIR) S.stash = S.phtab(3);  // after the three phase sets
+  S.init(L, smem, 2, (R)p.c1, (R)p.ch, threadIdx.x);
   const int Vs = L * L;
   const size_t sv = 2 * (size_t)Vs;  // reals per slice (vector and angles)
   const int rb = blockIdx.y;
@@ -80,48 +77,6 @@ __global__ void __launch_bounds__(MaxT<BY, EC>::value, MaxT<BY, EC>::min_blocks)
         S.store(z + t * sv, Y);
       }
       copy_blk<R, BY>(X0, X1);
-    }
-  } else if (PAIR) {  // OP_MHM, two B applications per block barrier
-    // With u_t = B_t x_t, y_{t+1} = x_{t+1} - sigma_t Cb u_t and
-    // (M^dag M x)_t = y_t - sigma_t Cb B_t y_{t+1}: B_t y_{t+1} (for output t)
-    // and u_{t+1} = B_{t+1} x_{t+1} (for y_{t+2}) are independent, so each
-    // factor of the two applications shares one exchange barrier.  Slice
-    // number i of the sequence tp, a, a+1, ... keeps its phases in set i % 3
-    // (written two applications after its set's last reader) and y in stash
-    // slot i % 2.
-    const int tp = (a - 1 + Nt) % Nt;
-    const int nT = b - a;
-    Cx<R> U[BY][2], Xn[BY][2];
-    if (S.on) {
-      S.load(X0, x + tp * sv);
-      S.load(X1, x + a * sv);
-    }
-    S.phases_into(phi + tp * sv, t1, th, 0);
-    S.phases_into(phi + a * sv, t1, th, 1);
-    copy_blk<R, BY>(U, X1);
-    if (S.on) S.load(Xn, x + ((a + 1) % Nt) * sv);
-    S.template applyB2<FAC_TILDE>(X0, S.phtab(0), U, S.phtab(1));  // u_tp, u_a
-    axpy_blk<R, BY>(Y, X1, sigma_of<R>(tp, Nt) * Cb, X0);          // y_a
-    S.park_to(Y, 1);
-    axpy_blk<R, BY>(Y, Xn, sigma_of<R>(a, Nt) * Cb, U);             // y_{a+1}
-    for (int i = 0; i < nT; ++i) {
-      const int t = a + i;
-      const bool more = t + 1 < b;  // u_{t+1} is needed for a later output
-      S.park_to(Y, i & 1);          // y_{t+1}: the next output's y_t
-      if (more) {
-        S.phases_into(phi + (t + 1) * sv, t1, th, (i + 2) % 3);
-        copy_blk<R, BY>(U, Xn);  // x_{t+1}
-        if (S.on) S.load(Xn, x + ((t + 2) % Nt) * sv);
-        S.template applyB2<FAC_TILDE>(Y, S.phtab((i + 1) % 3), U, S.phtab((i + 2) % 3));
-      } else {
-        S.template applyB1<FAC_TILDE>(Y, S.phtab((i + 1) % 3));
-      }
-      S.unpark_from(X0, (i + 1) & 1);  // y_t
-      if (S.on) {
-        axpy_blk<R, BY>(X0, X0, sigma_of<R>(t, Nt) * Cb, Y);  // y_t - sigma_t Cb B_t y_{t+1}
-        S.store(z + t * sv, X0);
-      }
-      if (more) axpy_blk<R, BY>(Y, Xn, sigma_of<R>(t + 1, Nt) * Cb, U);  // y_{t+2}
     }
   } else {  // OP_MHM
     // prologue: y_a = x_a - sigma_{a-1} B_{a-1} x_{a-1}
@@ -847,8 +802,7 @@ static size_t smem_limit() { return 227 * 1024; }
 template <typename R, typename A, int BY, int EC>
 static int launch_operator_t(int op, const OpArgs& a, cudaStream_t st) {
   const int threads = slice_threads(a.L, BY, (EC & EC_XS) != 0);
-  const size_t smem = (EC & EC_PAIR) ? pair_smem_bytes<R>(a.L, BY) : slice_smem_bytes<R, EC>(a.L, BY, 2);
-  if ((EC & EC_PAIR) && op != OP_MHM) return QEDF_ERR_ARG;
+  const size_t smem = slice_smem_bytes<R, EC>(a.L, BY, 2);
   if (smem > smem_limit() || threads > MaxT<BY, EC>::value) return QEDF_ERR_SIZE;
   dim3 grid((a.Nt + a.T - 1) / a.T, a.bs);
   if (op == OP_M) {
@@ -868,7 +822,7 @@ static int launch_operator_t(int op, const OpArgs& a, cudaStream_t st) {
 // L = 48); every other L runs the run-time-L engine.
 template <typename R, typename A, int BY, int EC>
 static int launch_operator_fl(int op, const OpArgs& a, cudaStream_t st) {
-  if constexpr (EC == 0 || EC == EC_PHS || EC == (EC_PAIR | EC_PHS))
+  if constexpr (EC == 0 || EC == EC_PHS)
     return with_fixed_l<BY>(a.L, [&](auto lt) {
       return launch_operator_t<R, A, BY, EC | EC_L(decltype(lt)::value)>(op, a, st);
     });
@@ -879,10 +833,6 @@ static int launch_operator_fl(int op, const OpArgs& a, cudaStream_t st) {
 // room for the stash, y stays in registers
 template <typename R, typename A, int BY>
 static int launch_operator_by(int op, const OpArgs& a, int xs, cudaStream_t st) {
-  // single-precision M^dag M: two B applications per barrier where the
-  // paired engine's shared memory fits
-  if (sizeof(R) == 4 && op == OP_MHM && pair_smem_bytes<R>(a.L, BY) <= smem_limit())
-    return launch_operator_fl<R, A, BY, EC_PAIR | EC_PHS>(op, a, st);
   if (sizeof(R) == 8 && slice_smem_bytes<R, EC_PHS>(a.L, BY, 2) <= smem_limit())
     return launch_operator_fl<R, A, BY, EC_PHS>(op, a, st);
   if (sizeof(R) == 4 && xs && xs_possible(a.L) && ((a.L / 2) & (a.L / 2 - 1)) == 0 &&

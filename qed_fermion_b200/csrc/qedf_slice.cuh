@@ -55,13 +55,9 @@ struct MaxThreads {
 //              no thread waits on a global load in the slice loop
 //   EC_BF16    (PCG, with EC_STAGE) the iteration vectors are stored as bf16
 //              pairs; the arithmetic stays in single precision
-//   EC_PAIR    (M^dag M) two B applications per block barrier: B_t on y_{t+1}
-//              together with B_{t+1} on x_{t+1}, each factor's exchange for
-//              both vectors around one barrier (factor2); phases of three
-//              slices in shared memory, two stash slots (pair_smem_bytes)
 //   EC_L(l)    (bits 8 and up) the lattice side fixed at compile time, so the
 //              engine's index arithmetic folds into constants; 0 = run-time L
-enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_STAGE = 8, EC_BF16 = 16, EC_PAIR = 32 };
+enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_STAGE = 8, EC_BF16 = 16 };
 __host__ __device__ constexpr int EC_L(int l) { return l << 8; }
 __host__ __device__ constexpr int ec_fixed_l(int ec) { return ec >> 8; }
 // Lattice sides with engines compiled for their size: the benchmark
@@ -118,13 +114,6 @@ __host__ __device__ inline size_t slice_smem_bytes(int L, int BY, int nbuf) {
   return sizeof(Cx<R>) * (nbuf * BY * NT + ph + ((EC & EC_NOSTASH) ? 0 : 2 * BY * NT));
 }
 
-// Shared memory of the paired engine: four exchange buffers, three phase sets
-// and two stash slots, 20 BY NT complex numbers.
-template <typename R>
-__host__ __device__ inline size_t pair_smem_bytes(int L, int BY) {
-  return sizeof(Cx<R>) * 20 * (size_t)BY * (L / 2) * (L / BY);
-}
-
 template <typename R, int BY, bool PHS = false, bool XS = false, int LT = 0>
 struct Slice {
   static_assert(BY % 2 == 0, "BY must be even");
@@ -158,7 +147,6 @@ struct Slice {
   // (r & ~1) + 1 (right column) of cross row r; y factors slot 0 (top row)
   // and slot 1 (bottom row)
   __device__ __forceinline__ Cx<R>* slot(Cx<R>* buf, int s) const { return buf + (size_t)s * NT; }
-  __device__ __forceinline__ const Cx<R>* slot(const Cx<R>* buf, int s) const { return buf + (size_t)s * NT; }
 
   // smem must hold slice_smem_bytes<R, EC>(L, BY, nbuf) for the kernel's EC
   __device__ void init(int L_, unsigned char* smem, int nbuf, R c1_, R ch_, int tid) {
@@ -438,162 +426,6 @@ struct Slice {
       }
     }
     if (BUF < 0) cur ^= 1;
-  }
-
-  // ---- two vectors per block barrier (the paired engine) --------------------
-  // Phase tables in sets of [4][BY][NT] (the PHS layout), set k at
-  // phtab(k); exchange buffers xb[0..1] for the first vector and xb[2..3] for
-  // the second; the stash holds two slots of one vector block each.
-  __device__ __forceinline__ Cx<R>* phtab(int k) const { return ph + (size_t)k * 4 * BY * NT; }
-  // all bonds' phases of one slice into set k (no barrier: a later block
-  // barrier must come before any thread reads them)
-  template <typename A>
-  __device__ __forceinline__ void phases_into(const A* ang, R t1, R th, int k) const {
-    if (!on) return;
-    Cx<R>* tb = phtab(k);
-#pragma unroll
-    for (int r = 0; r < BY; ++r) {
-      A a[4];
-      ld4(ang + 2 * ((y0 + r) * L + x0), a);
-      // x-bond of (x0+c, y0+r) is in g1 when the site is an A site, else g3
-      tb[(size_t)(0 * BY + r) * NT + id] = tphase((R)a[0], (r & 1) == 0 ? t1 : th);
-      tb[(size_t)(1 * BY + r) * NT + id] = tphase((R)a[1], th);
-      tb[(size_t)(2 * BY + r) * NT + id] = tphase((R)a[2], (r & 1) == 1 ? t1 : th);
-      tb[(size_t)(3 * BY + r) * NT + id] = tphase((R)a[3], th);
-    }
-  }
-  __device__ __forceinline__ void park_to(const Cx<R> (&v)[BY][2], int k) const {
-    if (!on) return;
-    Cx<R>* s = stash + (size_t)k * 2 * BY * NT;
-#pragma unroll
-    for (int r = 0; r < BY; ++r) {
-      s[(size_t)(2 * r) * NT + id] = v[r][0];
-      s[(size_t)(2 * r + 1) * NT + id] = v[r][1];
-    }
-  }
-  __device__ __forceinline__ void unpark_from(Cx<R> (&v)[BY][2], int k) const {
-    if (!on) return;
-    const Cx<R>* s = stash + (size_t)k * 2 * BY * NT;
-#pragma unroll
-    for (int r = 0; r < BY; ++r) {
-      v[r][0] = s[(size_t)(2 * r) * NT + id];
-      v[r][1] = s[(size_t)(2 * r + 1) * NT + id];
-    }
-  }
-  // the edge values a factor's neighbours need, into buffer buf
-  template <int G>
-  __device__ __forceinline__ void fexport(const Cx<R> (&v)[BY][2], Cx<R>* buf) const {
-    if (!on) return;
-    if (G == 0 || G == 2) {
-#pragma unroll
-      for (int r = 0; r < BY; ++r)
-        if (xcross(G, r)) {
-          slot(buf, r & ~1)[id] = v[r][0];
-          slot(buf, (r & ~1) + 1)[id] = v[r][1];
-        }
-    } else {
-      constexpr int CC = (G == 1) ? 1 : 0;
-      slot(buf, 0)[id] = v[0][CC];
-      slot(buf, 1)[id] = v[BY - 1][CC];
-    }
-  }
-  // the factor's update of the owned sites from old values, the neighbours'
-  // exported values in buf and the phase set tb (after a block barrier)
-  template <int G, int MODE>
-  __device__ __forceinline__ void fupdate(Cx<R> (&v)[BY][2], const Cx<R>* tb, const Cx<R>* buf) const {
-    if (!on) return;
-    const R c = (G == 0) ? c1 : ch;
-    auto tpx = [&](int r, int cc) { return tb[(size_t)(2 * cc * BY + r) * NT + id]; };
-    auto tpy = [&](int r, int cc) { return tb[(size_t)((2 * cc + 1) * BY + r) * NT + id]; };
-    if (G == 0 || G == 2) {
-#pragma unroll
-      for (int r = 0; r < BY; ++r) {
-        if (!xcross(G, r)) {
-          pair_update<MODE>(v[r][0], v[r][1], tpx(r, 0), c);
-        } else {
-          const Cx<R> right = slot(buf, r & ~1)[idr];
-          const Cx<R> left = slot(buf, (r & ~1) + 1)[idl];
-          Cx<R> ao = tpx(r, 1), al = tb[(size_t)(2 * BY + r) * NT + idl];
-          if (MODE == FAC_INV) {
-            ao = cneg(ao);
-            al = cneg(al);
-          }
-          v[r][1] = cfma(ao, right, v[r][1]);
-          v[r][0] = cjfma(al, left, v[r][0]);
-          if (MODE != FAC_TILDE) {
-            v[r][1] = c * v[r][1];
-            v[r][0] = c * v[r][0];
-          }
-        }
-      }
-    } else {
-      constexpr int CL = (G == 1) ? 0 : 1;
-      constexpr int CC = 1 - CL;
-#pragma unroll
-      for (int r = 0; r < BY; r += 2) pair_update<MODE>(v[r][CL], v[r + 1][CL], tpy(r, CL), c);
-#pragma unroll
-      for (int r = 1; r + 1 < BY; r += 2) pair_update<MODE>(v[r][CC], v[r + 1][CC], tpy(r, CC), c);
-      const Cx<R> below = slot(buf, 0)[idd];
-      const Cx<R> above = slot(buf, 1)[idu];
-      Cx<R> ab = tpy(BY - 1, CC), at = tb[(size_t)((2 * CC + 1) * BY + BY - 1) * NT + idu];
-      if (MODE == FAC_INV) {
-        ab = cneg(ab);
-        at = cneg(at);
-      }
-      Cx<R> nb = cfma(ab, below, v[BY - 1][CC]);
-      Cx<R> nt = cjfma(at, above, v[0][CC]);
-      if (MODE != FAC_TILDE) {
-        nb = c * nb;
-        nt = c * nt;
-      }
-      v[BY - 1][CC] = nb;
-      v[0][CC] = nt;
-    }
-  }
-  // factor G on v (phase set tv) and on w (phase set tw) around one barrier;
-  // the exchange buffers alternate with `cur`, so consecutive calls never
-  // write a buffer another thread may still read
-  template <int G, int MODE>
-  __device__ __forceinline__ void factor2(Cx<R> (&v)[BY][2], const Cx<R>* tv, Cx<R> (&w)[BY][2],
-                                          const Cx<R>* tw) {
-    Cx<R>* bv = cur ? xb[1] : xb[0];
-    Cx<R>* bw = cur ? xb[3] : xb[2];
-    fexport<G>(v, bv);
-    fexport<G>(w, bw);
-    __syncthreads();
-    fupdate<G, MODE>(v, tv, bv);
-    fupdate<G, MODE>(w, tw, bw);
-    cur ^= 1;
-  }
-  template <int G, int MODE>
-  __device__ __forceinline__ void factor1(Cx<R> (&v)[BY][2], const Cx<R>* tv) {
-    Cx<R>* bv = cur ? xb[1] : xb[0];
-    fexport<G>(v, bv);
-    __syncthreads();
-    fupdate<G, MODE>(v, tv, bv);
-    cur ^= 1;
-  }
-  // B (without Cb for FAC_TILDE) on two vectors with their own slices' phases
-  template <int MODE>
-  __device__ __forceinline__ void applyB2(Cx<R> (&v)[BY][2], const Cx<R>* tv, Cx<R> (&w)[BY][2],
-                                          const Cx<R>* tw) {
-    factor2<3, MODE>(v, tv, w, tw);
-    factor2<2, MODE>(v, tv, w, tw);
-    factor2<1, MODE>(v, tv, w, tw);
-    factor2<0, MODE>(v, tv, w, tw);
-    factor2<1, MODE>(v, tv, w, tw);
-    factor2<2, MODE>(v, tv, w, tw);
-    factor2<3, MODE>(v, tv, w, tw);
-  }
-  template <int MODE>
-  __device__ __forceinline__ void applyB1(Cx<R> (&v)[BY][2], const Cx<R>* tv) {
-    factor1<3, MODE>(v, tv);
-    factor1<2, MODE>(v, tv);
-    factor1<1, MODE>(v, tv);
-    factor1<0, MODE>(v, tv);
-    factor1<1, MODE>(v, tv);
-    factor1<2, MODE>(v, tv);
-    factor1<3, MODE>(v, tv);
   }
 
   // B = F4 F3 F2 F1 F2 F3 F4 without the scalar Cb (FAC_TILDE) or exact.
