@@ -631,6 +631,8 @@ def run_native(args):
             "fp64_plain": fp64, "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
             "speedup_vs_fp64_dropin": ((value / world) / fp64["dropin"]["value"]
                                        if fp64 and "dropin" in fp64 else None),
+            "pcg_launch_shape": ({k: hmc.solver.tuned[k] for k in ("by", "slab", "stage")}
+                                 if hmc.solver.tuned else None),
             "bf16": bf16, "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate,
             "acceptance_vs_fp64": acc, **result,
         }
@@ -817,6 +819,10 @@ def run_configs(args):
     def emit(d):
         print(json.dumps({"config_run": True, **d}), flush=True)
 
+    def tuned(solver):
+        t = solver.tuned
+        return None if t is None else {k: t[k] for k in ("by", "slab", "stage", "us_per_iter")}
+
     # C2: uniform angles, b = M^dag eta
     L, Lt = 24, 240
     N = L * L * Lt
@@ -832,11 +838,11 @@ def run_configs(args):
         emit({"config": "C2", "what": f"M^dag M {prec}, 1 rhs (a single launch of 138,240 sites)", "ms": ms,
               "GBps": bps * N / (ms / 1e3) / 1e9})
     for mode in ("mixed", "fp64"):
-        s = PcgSolver([System(L, Lt, 1)], mode=mode, rtol=1e-8, max_iter=100000, device=dev)
+        s = PcgSolver([System(L, Lt, 1)], mode=mode, rtol=1e-8, max_iter=100000, device=dev, tune=True)
         args_ = (phi.reshape(-1).to(s.angle_dtype), b.reshape(-1).to(s.vec_dtype))
         ms, res = timed(lambda: s.solve(*args_))
         emit({"config": "C2", "what": f"PCG to 1e-8, {mode}", "ms": ms, "iters": int(res.iters.max()),
-              "relres": float(res.relres.max()), "status": int(res.status.max())})
+              "relres": float(res.relres.max()), "status": int(res.status.max()), "tuned": tuned(s)})
 
     # C4a: 64 Z2 noise vectors sharing one L=36 field
     L, Lt, nrv = 36, 360, 64
@@ -845,7 +851,7 @@ def run_configs(args):
     eta = se.random_vec_bin()
     ms, _ = timed(lambda: se.set_eta_G_eta(bos, eta))
     emit({"config": "C4a", "what": "G_eta = (M^dag M)^-1 M^dag eta, 64 rhs, mixed, rtol 1e-10", "ms": ms,
-          "iters": int(se.iters.max()), "relres": float(se.relres.max())})
+          "iters": int(se.iters.max()), "relres": float(se.relres.max()), "tuned": tuned(se.solver)})
     ms, _ = timed(lambda: se.get_bond_bond_per_b2(bos))
     emit({"config": "C4a", "what": "bond-bond correlators T1+T21+T2+T4+Tvv over the 2016 noise pairs "
                                    "(complex128, cuFFT)", "ms": ms})
@@ -879,12 +885,12 @@ def run_configs(args):
     systems = [System(L, 10 * L, 1) for L in Ls]
     phis = [ref_to_kernel(torch.tensor(pi_flux_np(rng, L, 10 * L, 1), device=dev)).reshape(-1) for L in Ls]
     rhs = [torch.randn(10 * L ** 3, dtype=torch.complex128, device=dev) / math.sqrt(2) for L in Ls]
-    s = PcgSolver(systems, mode="mixed", rtol=1e-10, max_iter=20000, device=dev)
+    s = PcgSolver(systems, mode="mixed", rtol=1e-10, max_iter=20000, device=dev, tune=True)
     args_ = (torch.cat(phis).float(), torch.cat(rhs))
     ms, res = timed(lambda: s.solve(*args_))
     emit({"config": "C4b", "what": "16 uneven lattices, one launch, mixed, rtol 1e-10", "ms": ms,
           "iters_min": int(res.iters.min()), "iters_max": int(res.iters.max()),
-          "relres_max": float(res.relres.max())})
+          "relres_max": float(res.relres.max()), "tuned": tuned(s)})
 
     # C5: one 30-step trajectory at L=66, Ltau=660 (mixed)
     L, Lt = 66, 660
@@ -893,7 +899,8 @@ def run_configs(args):
     b0 = torch.tensor(pi_flux_np(rng, L, Lt, 1), dtype=torch.float32, device=dev)
     ms, out = timed(lambda: hmc.leapfrog_proposer5(b0))
     emit({"config": "C5", "what": "one trajectory, 30 leapfrog steps of 0.02, mixed, rtol 1e-10", "ms": ms,
-          "cg_iters_per_solve": float(out[3].float().mean()), "delta_H": float(out[2] - out[1])})
+          "cg_iters_per_solve": float(out[3].float().mean()), "delta_H": float(out[2] - out[1]),
+          "tuned": tuned(hmc.solver)})
     return 0
 
 
