@@ -167,6 +167,24 @@ int qedf_bb_kspace_acc_c64(const float* A, const float* B, int64_t rows, int Vs,
 int qedf_bb_kspace_acc_c128(const double* A, const double* B, int64_t rows, int Vs, double* S,
                             qedf_stream_t stream);
 
+/* Tvv (stochastic_estimator.py:1612-1652): writes each noise vector's current
+ * field v_s(r) = g_s(r+x) conj(eta_s(r)) e^{i phi_x} + g_s(r) conj(eta_s(r+x))
+ * e^{-i phi_x} for all slices ([Nrv][Ltau][Lx*Lx] complex) and adds its sum
+ * over vectors and slices to Tv[Lx*Lx] (complex128, double accumulation). */
+int qedf_bb_vfield_c64(const float* eta, const float* g_eta, const float* ephase, int Nrv, int Lx, int Ltau,
+                       float* v, double* Tv, qedf_stream_t stream);
+int qedf_bb_vfield_c128(const double* eta, const double* g_eta, const double* ephase, int Nrv, int Lx, int Ltau,
+                        double* v, double* Tv, qedf_stream_t stream);
+/* The short-distance terms T1, T21/T2 and T4 add to their pair sums (T1 :1440,
+ * T21 :1497, T4 :1605), summed over vectors, slices and sites into D[3]
+ * (complex128, double accumulation): D[0] = sum g(r+x) conj(eta(r-x))
+ * e^{i phi_x(r)} e^{i phi_x(r-x)}, D[1] = sum g(r) conj(eta(r)), D[2] = sum
+ * g(r) conj(eta(r+2x)) e^{-i phi_x(r)} e^{-i phi_x(r+x)}. */
+int qedf_bb_diag_c64(const float* eta, const float* g_eta, const float* ephase, int Nrv, int Lx, int Ltau,
+                     double* D, qedf_stream_t stream);
+int qedf_bb_diag_c128(const double* eta, const double* g_eta, const double* ephase, int Nrv, int Lx, int Ltau,
+                      double* D, qedf_stream_t stream);
+
 /* ---------------------------------------------------------------------------
  * Adaptive Fourier mass of the boson momenta (hmc_sampler_batch.py:1133-1277):
  * the arithmetic around the real FFTs over [Lx][Ly][Ltau] (the FFTs

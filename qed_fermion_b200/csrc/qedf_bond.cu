@@ -158,6 +158,100 @@ __global__ void __launch_bounds__(256) k_bb_kspace_acc(const R* A, const R* B, i
   }
 }
 
+// Tvv's current field of each noise vector s (stochastic_estimator.py:1612-1652),
+//   v_s(r) = g_s(r+x) conj(eta_s(r)) e^{i phi_x(r)} + g_s(r) conj(eta_s(r+x)) e^{-i phi_x(r)},
+// written for every slice, and its sum over vectors and slices per site,
+// added to Tv[Vs] (complex, double).  Grid (site blocks, vectors); a thread
+// walks its site through all slices, so the sum needs one atomic per site
+// and vector.
+template <typename R>
+__global__ void __launch_bounds__(256) k_bb_vfield(const R* eta, const R* g, const R* ep, int L, int Nt, R* v,
+                                                   double* Tv) {
+  const int Vs = L * L;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (r >= Vs) return;
+  const int x = r % L, y = r / L;
+  const int r1 = y * L + (x + 1 == L ? 0 : x + 1);
+  const int64_t base = (int64_t)s * Nt * Vs;
+  double sr = 0, si = 0;
+  for (int t = 0; t < Nt; ++t) {
+    const int64_t o = base + (int64_t)t * Vs;
+    const Cx<R> e = ldcx(ep, (int64_t)t * Vs + r);
+    const Cx<R> val = cmul(cmul(ldcx(g, o + r1), conjc(ldcx(eta, o + r))), e) +
+                      cmul(cmul(ldcx(g, o + r), conjc(ldcx(eta, o + r1))), conjc(e));
+    *reinterpret_cast<Cx<R>*>(v + 2 * (o + r)) = val;
+    sr += (double)val.re;
+    si += (double)val.im;
+  }
+  atomicAdd(Tv + 2 * r, sr);
+  atomicAdd(Tv + 2 * r + 1, si);
+}
+
+// The short-distance terms the correlators add to their pair sums, summed
+// over vectors, slices and sites into D[3] (complex, double):
+//   D[0] = sum g_s(r+x) conj(eta_s(r-x)) e^{i phi_x(r)} e^{i phi_x(r-x)}     (T1, at d = -x)
+//   D[1] = sum g_s(r) conj(eta_s(r))                                         (T21 and T2, at d = 0)
+//   D[2] = sum g_s(r) conj(eta_s(r+2x)) e^{-i phi_x(r)} e^{-i phi_x(r+x)}   (T4, at d = +x)
+template <typename R>
+__global__ void __launch_bounds__(256) k_bb_diag(const R* eta, const R* g, const R* ep, int Nrv, int L, int Nt,
+                                                 double* D) {
+  __shared__ double red[6][8];
+  const int Vs = L * L;
+  const int64_t n = (int64_t)Nrv * Nt * Vs;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(i % Vs);
+    const int64_t st = i - r;  // (vector, slice) offset
+    const int tslice = (int)((i / Vs) % Nt);
+    const int x = r % L, y = r / L;
+    const int xm = x == 0 ? L - 1 : x - 1, xp = x + 1 == L ? 0 : x + 1, xpp = xp + 1 == L ? 0 : xp + 1;
+    const int64_t et = (int64_t)tslice * Vs;
+    const Cx<R> e = ldcx(ep, et + r), em1 = ldcx(ep, et + y * L + xm), ep1 = ldcx(ep, et + y * L + xp);
+    const Cx<R> gr = ldcx(g, i);
+    const Cx<R> d0 = cmul(cmul(ldcx(g, st + y * L + xp), conjc(ldcx(eta, st + y * L + xm))), cmul(e, em1));
+    const Cx<R> d1 = cmul(gr, conjc(ldcx(eta, i)));
+    const Cx<R> d2 = cmul(cmul(gr, conjc(ldcx(eta, st + y * L + xpp))), conjc(cmul(e, ep1)));
+    acc[0] += d0.re;
+    acc[1] += d0.im;
+    acc[2] += d1.re;
+    acc[3] += d1.im;
+    acc[4] += d2.re;
+    acc[5] += d2.im;
+  }
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (ln == 0) red[k][w] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double v = 0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) v += red[threadIdx.x][q];
+    atomicAdd(D + threadIdx.x, v);
+  }
+}
+
+template <typename R>
+int vfield_entry(const R* eta, const R* g, const R* ep, int Nrv, int Lx, int Ltau, R* v, double* Tv,
+                 cudaStream_t st) {
+  if (!eta || !g || !ep || !v || !Tv || Nrv < 1 || Nrv > 65535 || Lx < 2 || Ltau < 1) return QEDF_ERR_ARG;
+  const int Vs = Lx * Lx;
+  k_bb_vfield<R><<<dim3((Vs + 255) / 256, Nrv), 256, 0, st>>>(eta, g, ep, Lx, Ltau, v, Tv);
+  return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
+}
+
+template <typename R>
+int diag_entry(const R* eta, const R* g, const R* ep, int Nrv, int Lx, int Ltau, double* D, cudaStream_t st) {
+  if (!eta || !g || !ep || !D || Nrv < 1 || Lx < 3 || Ltau < 1) return QEDF_ERR_ARG;
+  const int64_t n = (int64_t)Nrv * Ltau * Lx * Lx;
+  const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 4);
+  k_bb_diag<R><<<(unsigned)blocks, 256, 0, st>>>(eta, g, ep, Nrv, Lx, Ltau, D);
+  return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
+}
+
 template <typename R>
 int pair_fields_entry(int kind, const R* eta, const R* g, const R* ep, const int* ps, const int* pt, int npairs,
                       int Nrv, int Lx, int Ltau, R* fa, R* fb, cudaStream_t st) {
@@ -219,6 +313,22 @@ int qedf_bb_kspace_acc_c64(const float* A, const float* B, int64_t rows, int Vs,
 int qedf_bb_kspace_acc_c128(const double* A, const double* B, int64_t rows, int Vs, double* S,
                             qedf_stream_t s) {
   return kspace_acc_entry<double>(A, B, rows, Vs, S, reinterpret_cast<cudaStream_t>(s));
+}
+int qedf_bb_vfield_c64(const float* eta, const float* g_eta, const float* ephase, int Nrv, int Lx, int Ltau,
+                       float* v, double* Tv, qedf_stream_t s) {
+  return vfield_entry<float>(eta, g_eta, ephase, Nrv, Lx, Ltau, v, Tv, reinterpret_cast<cudaStream_t>(s));
+}
+int qedf_bb_vfield_c128(const double* eta, const double* g_eta, const double* ephase, int Nrv, int Lx, int Ltau,
+                        double* v, double* Tv, qedf_stream_t s) {
+  return vfield_entry<double>(eta, g_eta, ephase, Nrv, Lx, Ltau, v, Tv, reinterpret_cast<cudaStream_t>(s));
+}
+int qedf_bb_diag_c64(const float* eta, const float* g_eta, const float* ephase, int Nrv, int Lx, int Ltau,
+                     double* D, qedf_stream_t s) {
+  return diag_entry<float>(eta, g_eta, ephase, Nrv, Lx, Ltau, D, reinterpret_cast<cudaStream_t>(s));
+}
+int qedf_bb_diag_c128(const double* eta, const double* g_eta, const double* ephase, int Nrv, int Lx, int Ltau,
+                      double* D, qedf_stream_t s) {
+  return diag_entry<double>(eta, g_eta, ephase, Nrv, Lx, Ltau, D, reinterpret_cast<cudaStream_t>(s));
 }
 
 }  // extern "C"

@@ -35,20 +35,6 @@ class BondBond:
         self.chunk_bytes = int(chunk_bytes)
 
     # ---- helpers ----------------------------------------------------------
-    def _fields(self, eta, G_eta, boson):
-        for t in (eta, G_eta, boson):
-            if not t.is_cuda:
-                raise RuntimeError("bond-bond correlators need CUDA tensors")
-        ec = eta.conj().reshape(-1, self.Ltau, self.Ly, self.Lx)
-        g = G_eta.reshape(-1, self.Ltau, self.Ly, self.Lx).to(ec.dtype)
-        ph = boson.permute(0, 1, 4, 3, 2)[0, 0].to(ec.real.dtype)  # [Ltau, Ly, Lx], x-bond angles
-        return ec, g, ph
-
-    @staticmethod
-    def _sx(a, k):
-        """value at x + k (the reference's torch.roll(a, shifts=-k, dims=-1))"""
-        return torch.roll(a, shifts=-k, dims=-1)
-
     def _chunk(self, ec, n_arrays=4):
         per = ec[0].numel() * ec.element_size() * n_arrays
         return max(1, self.chunk_bytes // max(1, per))
@@ -79,19 +65,29 @@ class BondBond:
         S = S.view(self.Ly, self.Lx) / (Vs * Vs)
         return (torch.fft.ifft2(S, norm="forward") / (len(pairs) * self.Ltau)).to(dt)
 
+    def _inputs(self, eta, G_eta, boson):
+        """eta, G_eta as contiguous [Nrv, N] of one dtype and e^{i phi_x} [Ltau, Ly, Lx]."""
+        dt = eta.dtype
+        nrv = eta.shape[0]
+        e = eta.resolve_conj().reshape(nrv, -1).contiguous()
+        g = G_eta.to(dt).resolve_conj().reshape(nrv, -1).contiguous()
+        ph = boson.permute(0, 1, 4, 3, 2)[0, 0].to(e.real.dtype)
+        return e, g, torch.exp(1j * ph).to(dt).contiguous()
+
+    def _diag(self, eta, G_eta, boson):
+        """The three short-distance terms as means (kernel ``bb_diag``)."""
+        e, g, ep = self._inputs(eta, G_eta, boson)
+        return ops.bb_diag(e, g, ep, self.Lx) / e.numel()
+
     # ---- the correlators ----------------------------------------------------
     def T1(self, eta, G_eta, boson):
-        ec, g, ph = self._fields(eta, G_eta, boson)
-        e = torch.exp(1j * ph)
-        sx = self._sx
         out = -self._pair_mean("T1", eta, G_eta, boson)
-        out[0, -1] += (sx(g, 1) * torch.roll(ec, 1, dims=-1) * e * torch.exp(1j * torch.roll(ph, 1, dims=-1))).mean()
+        out[0, -1] += self._diag(eta, G_eta, boson)[0].to(out.dtype)
         return out
 
     def T21(self, eta, G_eta, boson):
-        ec, g, ph = self._fields(eta, G_eta, boson)
         out = -self._pair_mean("T21", eta, G_eta, boson)
-        out[0, 0] += (g * ec).mean()
+        out[0, 0] += self._diag(eta, G_eta, boson)[1].to(out.dtype)
         return out
 
     @staticmethod
@@ -108,31 +104,37 @@ class BondBond:
 
     def T2_direct(self, eta, G_eta, boson):
         """T2 from its own pair fields (the reference's computation)."""
-        ec, g, ph = self._fields(eta, G_eta, boson)
         out = -self._pair_mean("T2", eta, G_eta, boson)
-        out[0, 0] += (g * ec).mean()
+        out[0, 0] += self._diag(eta, G_eta, boson)[1].to(out.dtype)
         return out
 
     def T4(self, eta, G_eta, boson):
-        ec, g, ph = self._fields(eta, G_eta, boson)
-        e = torch.exp(-1j * ph)
-        sx = self._sx
         out = -self._pair_mean("T4", eta, G_eta, boson)
-        out[0, 1] += (g * sx(ec, 2) * e * torch.exp(-1j * sx(ph, 1))).mean()
+        out[0, 1] += self._diag(eta, G_eta, boson)[2].to(out.dtype)
         return out
 
     def Tvv(self, eta, G_eta, boson):
-        ec, g, ph = self._fields(eta, G_eta, boson)
-        sx = self._sx
-        ep, em = torch.exp(1j * ph), torch.exp(-1j * ph)
-        S = torch.zeros((self.Ly, self.Lx), dtype=ec.dtype, device=ec.device)
-        Tv = torch.zeros((self.Ly, self.Lx), dtype=ec.dtype, device=ec.device)
-        nrv = ec.shape[0]
-        for idx in torch.arange(nrv, device=ec.device).split(self._chunk(ec, 3)):
-            v = sx(g[idx], 1) * ec[idx] * ep + g[idx] * sx(ec[idx], 1) * em
-            S += (torch.fft.ifft2(v, norm="backward") * torch.fft.fft2(v, norm="forward")).sum(dim=(0, 1))
-            Tv += v.sum(dim=(0, 1))
-        return torch.fft.ifft2(S, norm="forward") / (nrv * self.Ltau), Tv / (nrv * self.Ltau)
+        """The current-current correlation and the mean current: each vector's
+        field v (kernel ``bb_vfield``, which also sums it), the products of its
+        transforms summed in k-space (``bb_kspace_acc``), one inverse FFT."""
+        e, g, ep = self._inputs(eta, G_eta, boson)
+        nrv = e.shape[0]
+        Vs = self.Lx * self.Ly
+        S = torch.zeros(Vs, dtype=torch.complex128, device=e.device)
+        Tv = torch.zeros(Vs, dtype=torch.complex128, device=e.device)
+        per = max(1, self.chunk_bytes // max(1, 3 * e[0].numel() * e.element_size()))
+        v = torch.empty((min(per, nrv), self.Ltau, self.Ly, self.Lx), dtype=e.dtype, device=e.device)
+        for lo in range(0, nrv, per):
+            n = min(per, nrv - lo)
+            vb = v[:n]
+            ops.bb_vfield(e[lo:lo + n], g[lo:lo + n], ep, self.Lx, vb, Tv)
+            # the reference's ifft2(v, "backward") * fft2(v, "forward"): unnormalised
+            # transforms here, their two 1 / Vs applied to the sum once
+            ops.bb_kspace_acc(torch.fft.ifft2(vb, norm="forward"), torch.fft.fft2(vb, norm="backward"), S)
+        S = S.view(self.Ly, self.Lx) / (Vs * Vs)
+        dt = eta.dtype
+        return ((torch.fft.ifft2(S, norm="forward") / (nrv * self.Ltau)).to(dt),
+                (Tv.view(self.Ly, self.Lx) / (nrv * self.Ltau)).to(dt))
 
     def get_bond_bond_per_b2(self, eta, G_eta, boson):
         """BB0_r, BB_r, B_r and BB_k (real parts; BB_k in ascending momentum order)."""

@@ -194,6 +194,45 @@ def bb_kspace_acc(A: torch.Tensor, B: torch.Tensor, S: torch.Tensor) -> None:
     _lib.call(f"qedf_bb_kspace_acc_{prec}", ptr(A), ptr(B), A.numel() // Vs, Vs, ptr(S), stream_handle())
 
 
+def _bb_inputs(name, eta, g_eta, ephase, Lx):
+    _check_cuda(eta, g_eta, ephase)
+    prec, _ = _PREC[eta.dtype]
+    for t in (g_eta, ephase):
+        if t.dtype != eta.dtype or not t.is_contiguous() or t.is_conj():
+            raise RuntimeError(f"{name}: complex tensors must share eta's dtype and be contiguous")
+    if eta.dim() != 2 or not eta.is_contiguous() or eta.is_conj():
+        raise RuntimeError(f"{name}: eta must be a contiguous [Nrv, Ltau * Lx^2]")
+    nrv, N = eta.shape
+    Vs, Ltau = lattice_dims(N, Lx)
+    if g_eta.numel() != eta.numel() or ephase.numel() != N:
+        raise RuntimeError(f"{name}: buffer sizes do not match")
+    return prec, nrv, N, Vs, Ltau
+
+
+def bb_vfield(eta: torch.Tensor, g_eta: torch.Tensor, ephase: torch.Tensor, Lx: int, v: torch.Tensor,
+              Tv: torch.Tensor) -> None:
+    """Tvv's current field of every noise vector into ``v`` (eta's shape and
+    dtype) and its sum over vectors and slices added to the complex128 ``Tv``
+    of Lx^2 entries."""
+    prec, nrv, N, Vs, Ltau = _bb_inputs("bb_vfield", eta, g_eta, ephase, Lx)
+    _check_cuda(v, Tv)
+    if v.dtype != eta.dtype or v.numel() != eta.numel() or not v.is_contiguous():
+        raise RuntimeError("bb_vfield: v must be a contiguous buffer like eta")
+    if Tv.dtype != torch.complex128 or Tv.numel() != Vs or not Tv.is_contiguous():
+        raise RuntimeError("bb_vfield: Tv must be a contiguous complex128 buffer of Lx^2 entries")
+    _lib.call(f"qedf_bb_vfield_{prec}", ptr(eta), ptr(g_eta), ptr(ephase), nrv, Lx, Ltau, ptr(v), ptr(Tv),
+              stream_handle())
+
+
+def bb_diag(eta: torch.Tensor, g_eta: torch.Tensor, ephase: torch.Tensor, Lx: int) -> torch.Tensor:
+    """The short-distance terms of T1, T21/T2 and T4 summed over vectors,
+    slices and sites (complex128 [3]; divide by their count for the means)."""
+    prec, nrv, N, Vs, Ltau = _bb_inputs("bb_diag", eta, g_eta, ephase, Lx)
+    D = torch.zeros(3, dtype=torch.complex128, device=eta.device)
+    _lib.call(f"qedf_bb_diag_{prec}", ptr(eta), ptr(g_eta), ptr(ephase), nrv, Lx, Ltau, ptr(D), stream_handle())
+    return D
+
+
 def _rprec(t):
     if t.dtype == torch.float32:
         return "f32"
