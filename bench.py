@@ -89,6 +89,8 @@ def parse_args(argv=None):
                     help="only time M^dag M on this many right-hand sides (c64; c128 with --mode fp64)")
     ap.add_argument("--mode", default="mixed", choices=["mixed", "mixed_bf16", "fp32", "fp64"],
                     help="precision of the --solve-only solve or --matvec-only launch")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="the library's static launch shapes instead of the autotuner's timed choice")
     ap.add_argument("--quick", action="store_true",
                     help="timed trajectories only (no e2e, FP64, Delta H, matvec or CPU legs): for profiling")
     return ap.parse_args(argv)
@@ -347,7 +349,7 @@ def run_native(args):
     def make(precision, solver_impl="persistent"):
         h = HmcSampler(Lx=L, Ltau=Lt, J=1.0, K=1.0, dtau=0.1, bs=bs, delta_t=args.delta_t,
                        N_leapfrog=args.n_leapfrog, precision=precision, cg_rtol=args.rtol, max_iter=20000,
-                       device=dev, seed=seed, solver_impl=solver_impl)
+                       device=dev, seed=seed, solver_impl=solver_impl, autotune=args.autotune)
         return h
 
     hmc = make("mixed")

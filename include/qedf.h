@@ -249,8 +249,7 @@ typedef struct {
 #define QEDF_PCG_MIXED_BF16 3 /* as QEDF_PCG_MIXED, with the search direction p and the
                                  preconditioned residual z stored as bf16 pairs (4 bytes
                                  per complex number); r, M^dag M p and the float part of x
-                                 stay float, as does the arithmetic; lattices whose slice
-                                 stages fit in shared memory */
+                                 stay float, as does the arithmetic */
 
 typedef struct {
   int mode;           /* QEDF_PCG_* */
@@ -273,8 +272,7 @@ typedef struct {
                          -1: no window and no extra kernel */
   int stage;          /* 1: the operator passes stage their input slices in shared memory by
                          bulk copies where the stages fit (single-precision iterations);
-                         0 (default) or -1: the engine that loads them directly.  The
-                         MIXED_BF16 mode always stages. */
+                         0 (default) or -1: the engine that loads them directly */
 } qedf_pcg_opts;
 
 /* Bytes of device workspace qedf_pcg_solve needs for these systems. */

@@ -148,7 +148,7 @@ def pcg_choice(systems, mode, use_precon=True, dtau=0.1, iters=30, force=False) 
         if hit is not None:
             return hit
     device = torch.device("cuda", torch.cuda.current_device())
-    stages = [True, False] if mode in ("mixed", "fp32") else [True]
+    stages = [True, False] if mode in ("mixed", "fp32", "mixed_bf16") else [False]
     cands = [(by, T, st) for by in tile_heights([s.Lx for s in systems]) for T in slab_candidates(systems)
              for st in stages]
     phi = b = None

@@ -219,13 +219,13 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   constexpr bool STG_S = (ECS & EC_STAGE) != 0;
   static_assert(!STG_S || (STASH_S && !XS_S), "the staged engine keeps y_t in the stash");
   // storage of the search direction p and the preconditioned residual z: the
-  // iteration precision, or bf16 pairs (EC_BF16, staged engine, mixed mode).
+  // iteration precision, or bf16 pairs (EC_BF16, mixed mode).
   // r, M^dag M p and x_lo always keep the iteration precision, so that the
   // residual recurrence r -= alpha M^dag M p stays that of x += alpha p.
   constexpr bool BF = (ECS & EC_BF16) != 0;
   using SP = typename std::conditional<BF, bf16, RS>::type;
-  static_assert(!BF || (STG_S && sizeof(RS) == 4 && !std::is_same<RS, RH>::value),
-                "bf16 storage is a mixed-precision mode of the staged engine");
+  static_assert(!BF || (sizeof(RS) == 4 && !std::is_same<RS, RH>::value && !XS_S),
+                "bf16 storage is a mixed-precision mode");
   extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ RhsState st;
   __shared__ unsigned long long stg_bar[2];
@@ -464,9 +464,9 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const bool pend = st.pending[v];
     const RS al_old = (RS)st.alpha[v];
     RS* xl = xs + vb;
-    const RS* pold = reinterpret_cast<const RS*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
-    RS* pnew = reinterpret_cast<RS*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
-    const RS* zz = (S.precon ? zbuf : reinterpret_cast<const RS*>(r)) + vb;
+    const SP* pold = reinterpret_cast<const SP*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
+    SP* pnew = reinterpret_cast<SP*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
+    const SP* zz = ((S.precon || BF) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
     RS* O = Op + vb;
     const RS t1 = (RS)p.t1, th = (RS)p.th, Cb = (RS)p.Cb;
     Cx<RS> X0[BY][2], X1[BY][2], Y[BY][2];
@@ -474,10 +474,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     double pap = 0;
     auto getp = [&](Cx<RS> (&X)[BY][2], int t, bool own) {
       if (!E.on) return;
-      E.load_coherent(X, zz + t * sv);
+      E.load_st(X, zz + t * sv);
       if (has_old) {
         Cx<RS> T0[BY][2];
-        E.load_coherent(T0, pold + t * sv);
+        E.load_st(T0, pold + t * sv);
         if (own && pend) {
           Cx<RS> XL[BY][2];
           E.load_coherent(XL, xl + t * sv);
@@ -496,13 +496,14 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
           for (int c = 0; c < 2; ++c) {
             X[q][c].re = fma(beta, T0[q][c].re, X[q][c].re);
             X[q][c].im = fma(beta, T0[q][c].im, X[q][c].im);
+            X[q][c] = round_st<SP>(X[q][c]);
           }
       }
     };
     const int tp = (a - 1 + Nt) % Nt;
     getp(X0, tp, false);
     getp(X1, a, true);
-    if (E.on) E.store(pnew + a * sv, X1);
+    if (E.on) E.store_st(pnew + a * sv, X1);
     A ang[BY][4];
     if constexpr (!PHS_S) E.load_angles(ang, phi + a * sv);
     E.phases(phi + tp * sv, t1, th);
@@ -513,7 +514,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     for (int t = a; t < bnd; ++t) {
       const int tn = (t + 1) % Nt;
       getp(X1, tn, t + 1 < bnd);
-      if (E.on && t + 1 < bnd) E.store(pnew + tn * sv, X1);
+      if (E.on && t + 1 < bnd) E.store_st(pnew + tn * sv, X1);
       if constexpr (!PHS_S) {
         E.phases_from(ang, t1, th);
         if (t + 1 < bnd) E.load_angles(ang, phi + (t + 1) * sv);
@@ -1341,12 +1342,13 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
         return launch_pcg_fl<float, double, float, BY, 0, 0>(p, st);
       return launch_pcg_t<float, double, float, BY, 0, EC_NOSTASH>(p, st);
     case QEDF_PCG_MIXED_BF16:
-      // bf16 storage exists for the staged engine only
-      if (fits_staged<float, 0>(Lmax, BY) && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
+      if (p.stage && fits_staged<float, 0>(Lmax, BY) && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
         return launch_pcg_fl<float, double, float, BY, EC_STAGE | EC_BF16, EC_PHS>(p, st);
-      if (fits_staged<float, 0>(Lmax, BY) && fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
-        return launch_pcg_fl<float, double, float, BY, EC_STAGE | EC_BF16, 0>(p, st);
-      return QEDF_ERR_SIZE;
+      if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
+        return launch_pcg_fl<float, double, float, BY, EC_BF16, EC_PHS>(p, st);
+      if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
+        return launch_pcg_fl<float, double, float, BY, EC_BF16, 0>(p, st);
+      return launch_pcg_t<float, double, float, BY, EC_BF16, EC_NOSTASH>(p, st);
   }
   return QEDF_ERR_ARG;
 }

@@ -53,8 +53,9 @@ struct MaxThreads {
 //   EC_STAGE   the vector slices an operator pass reads are staged whole in
 //              shared memory by bulk copies one slice ahead (SliceStages), so
 //              no thread waits on a global load in the slice loop
-//   EC_BF16    (PCG, with EC_STAGE) the iteration vectors are stored as bf16
-//              pairs; the arithmetic stays in single precision
+//   EC_BF16    (PCG, mixed mode) the search direction p and the preconditioned
+//              residual z are stored as bf16 pairs; the arithmetic stays in
+//              single precision
 //   EC_L(l)    (bits 8 and up) the lattice side fixed at compile time, so the
 //              engine's index arithmetic folds into constants; 0 = run-time L
 enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_STAGE = 8, EC_BF16 = 16 };

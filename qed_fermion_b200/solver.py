@@ -76,8 +76,7 @@ class PcgSolver:
     ``stage`` lets the single-precision operator passes stage their input
     slices in shared memory by bulk copies where the stages fit (the results
     are the same bit for bit; measured no faster on the benchmark lattice, so
-    off by default and left to the autotuner).  The "mixed_bf16" mode always
-    stages.
+    off by default and left to the autotuner).
     """
 
     def __init__(self, systems: Sequence[System], mode: str = "mixed", rtol: float = 1e-10,
