@@ -633,7 +633,7 @@ def run_native(args):
             "fp64_plain": fp64, "speedup_vs_fp64": (value / world) / fp64["value"] if fp64 else None,
             "speedup_vs_fp64_dropin": ((value / world) / fp64["dropin"]["value"]
                                        if fp64 and "dropin" in fp64 else None),
-            "pcg_launch_shape": ({k: hmc.solver.tuned[k] for k in ("by", "slab", "stage")}
+            "pcg_launch_shape": ({k: hmc.solver.tuned[k] for k in ("by", "slab", "stage", "chunk")}
                                  if hmc.solver.tuned else None),
             "bf16": bf16, "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate,
             "acceptance_vs_fp64": acc, **result,
@@ -823,7 +823,7 @@ def run_configs(args):
 
     def tuned(solver):
         t = solver.tuned
-        return None if t is None else {k: t[k] for k in ("by", "slab", "stage", "us_per_iter")}
+        return None if t is None else {k: t[k] for k in ("by", "slab", "stage", "chunk", "us_per_iter")}
 
     # C2: uniform angles, b = M^dag eta
     L, Lt = 24, 240

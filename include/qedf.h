@@ -259,7 +259,8 @@ typedef struct {
   int use_precon;     /* builtin tau-banded preconditioner (systems with Ltau >= 26) */
   int ru_interval;    /* mixed: reliable update at least every ru_interval iterations */
   double ru_delta;    /* mixed: and whenever the residual fell by this factor */
-  int by, slab, chunk;/* tile choice, 0 = automatic */
+  int by, slab, chunk;/* tile height (2, 4, 6), tau-slab length of the operator units, sites
+                         per elementwise unit (16 or 32); 0 = automatic */
   double timeout_ms;  /* per grid-barrier wait, 0 = 2000 ms */
   long long* profile; /* optional device array of 8 counters (zeroed by the caller) that
                          accumulate SM clock cycles of block 0: 0 init, 1 operator phases,

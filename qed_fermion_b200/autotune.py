@@ -9,7 +9,7 @@ device once per problem shape and remembered:
   operator units (the library's load-balance search, or explicit lengths that
   give one, two or three rounds of units per thread block), and the engine
   that stages its input slices in shared memory against the one that loads
-  them directly.
+  them directly, and 16- or 32-site elementwise units.
 * M^dag M (``qedf_mhm_vec_*``): tile height and slab length.
 
 Each candidate runs a short fixed-iteration solve (or a few operator
@@ -149,14 +149,15 @@ def pcg_choice(systems, mode, use_precon=True, dtau=0.1, iters=30, force=False) 
             return hit
     device = torch.device("cuda", torch.cuda.current_device())
     stages = [True, False] if mode in ("mixed", "fp32", "mixed_bf16") else [False]
-    cands = [(by, T, st) for by in tile_heights([s.Lx for s in systems]) for T in slab_candidates(systems)
-             for st in stages]
+    chunks = [16, 32] if mode != "fp64" and max(s.Ltau for s in systems) <= 500 else [16]
+    cands = [(by, T, st, ch) for by in tile_heights([s.Lx for s in systems]) for T in slab_candidates(systems)
+             for st in stages for ch in chunks]
     phi = b = None
     timings = []
-    for by, T, st in cands:
+    for by, T, st, ch in cands:
         try:
             s = PcgSolver(systems, mode=mode, rtol=0.0, max_iter=iters, dtau=dtau, use_precon=use_precon,
-                          by=by, slab=T, stage=st, device=device, tune=False)
+                          by=by, slab=T, stage=st, chunk=ch, device=device, tune=False)
         except (ValueError, _lib.QedfError):
             continue
         if phi is None:
@@ -165,13 +166,18 @@ def pcg_choice(systems, mode, use_precon=True, dtau=0.1, iters=30, force=False) 
             ms = _time(lambda: s.solve(phi, b), reps=2)
         except _lib.QedfError:
             continue  # a shape this launch cannot take (shared memory, threads)
-        timings.append({"by": by, "slab": T, "stage": st, "us_per_iter": 1e3 * ms / iters})
+        timings.append({"by": by, "slab": T, "stage": st, "chunk": ch, "us_per_iter": 1e3 * ms / iters})
         del s
     if not timings:
-        raise RuntimeError(f"no PCG launch shape works for {shape}")
+        # no launch shape takes this batch (e.g. a lattice beyond the slice
+        # engine's limit): the library's defaults stand, and its solve reports
+        # the limit as it would without tuning
+        out = {"by": 0, "slab": 0, "stage": False, "chunk": 0, "us_per_iter": None, "candidates": []}
+        _remember(key, out)
+        return out
     best = min(timings, key=lambda t: t["us_per_iter"])
-    out = {"by": best["by"], "slab": best["slab"], "stage": best["stage"], "us_per_iter": best["us_per_iter"],
-           "candidates": timings}
+    out = {"by": best["by"], "slab": best["slab"], "stage": best["stage"], "chunk": best["chunk"],
+           "us_per_iter": best["us_per_iter"], "candidates": timings}
     _remember(key, out)
     return out
 
@@ -208,6 +214,10 @@ def operator_choice(L, Ltau, nvec, dtype, rhs_per_boson=1, force=False) -> dict:
             except _lib.QedfError:
                 continue
             timings.append({"by": by, "slab": T, "ms": ms})
+    if not timings:
+        res = {"by": 0, "slab": 0, "ms": None, "candidates": []}
+        _remember(key, res)
+        return res
     best = min(timings, key=lambda t: t["ms"])
     res = {"by": best["by"], "slab": best["slab"], "ms": best["ms"], "candidates": timings}
     _remember(key, res)

@@ -90,7 +90,7 @@ int launch_cdot(const R* u, const R* v, int64_t n, int rows, double* out, cudaSt
 // ---- persistent PCG -------------------------------------------------------
 constexpr int PCG_MAX_SYS = 32;
 constexpr int PCG_MAX_RHS = 256;
-constexpr int PCG_CHUNK = 16;  // sites per elementwise unit (a multiple of 2)
+constexpr int PCG_CHUNK = 16;  // sites per elementwise unit where 32 does not fit (a multiple of 2)
 
 struct PcgSys {
   int L, Nt, nrhs, shared;

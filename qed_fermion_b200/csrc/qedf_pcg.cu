@@ -245,9 +245,9 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   RH* xh = reinterpret_cast<RH*>(p.x);
   const RH* bvec = reinterpret_cast<const RH*>(p.b);
   const A* phi_all = reinterpret_cast<const A*>(p.phi);
-  constexpr int CH = PCG_CHUNK;   // sites per elementwise unit
-  constexpr int CHC = PCG_CHUNK;
-  constexpr int PPR = CHC / 2;    // site pairs per row of a unit
+  const int CH = p.CH;   // sites per elementwise unit (16 or 32)
+  const int CHC = CH;
+  const int PPR = CHC / 2;  // site pairs per row of a unit
 
   // slice stages of the operator passes (EC_STAGE): two buffers of z, p_old
   // and x_lo slices behind the slice engine's tables
@@ -1027,8 +1027,14 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
   p.xs = 1;
   p.stage = o->stage > 0 ? 1 : 0;
   p.l2 = o->l2_persist < 0 ? -1 : 0;
-  if (o->chunk != 0 && o->chunk != PCG_CHUNK) return QEDF_ERR_ARG;
-  p.CH = PCG_CHUNK;
+  if (o->chunk != 0 && o->chunk != 16 && o->chunk != 32) return QEDF_ERR_ARG;
+  // 32-site elementwise units (one longer tau column per block) where their r
+  // column and the single-precision staging fit in shared memory next to the
+  // per-block state, else 16
+  int ntmax_all = 0;
+  for (int s = 0; s < nsys; ++s) ntmax_all = std::max(ntmax_all, sys[s].Ltau);
+  const bool wide_fits = o->mode != QEDF_PCG_PLAIN_F64 && ntmax_all <= 500;
+  p.CH = o->chunk ? o->chunk : (wide_fits ? 32 : PCG_CHUNK);
   const int nblk = num_sms();
   int rhs = 0, ua = 0, ue = 0, pt = 0;
   int64_t vec = 0, phi = 0;
@@ -1236,7 +1242,7 @@ static int launch_pcg_t(PcgParams& p, cudaStream_t st) {
   smem = std::max(smem, slice_smem_bytes<RH, ECH>(Lmax, BY, 2));
   // elementwise units: the r column, and in single precision the staging
   // area of the update pass
-  smem = std::max(smem, ((sizeof(Cx<RS>) * (size_t)Ntmax * PCG_CHUNK + 15) / 16 * 16) +
+  smem = std::max(smem, ((sizeof(Cx<RS>) * (size_t)Ntmax * p.CH + 15) / 16 * 16) +
                             (sizeof(RS) == 4 ? PCG_EW_STAGES * 2 * 16 * (size_t)threads : 0));
   if (smem + sizeof(RhsState) > 227 * 1024) return QEDF_ERR_SIZE;
   auto kern = k_pcg<RS, RH, A, BY, ECS, ECH>;

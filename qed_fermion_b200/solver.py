@@ -96,6 +96,7 @@ class PcgSolver:
             with torch.cuda.device(self.device):
                 self.tuned = autotune.pcg_choice(self.systems, mode, use_precon=use_precon, dtau=dtau)
             by, slab, stage = self.tuned["by"], self.tuned["slab"], self.tuned["stage"]
+            chunk = self.tuned.get("chunk", chunk)
         n = len(self.systems)
         self._sys = (_lib.QedfSystem * n)(*[_lib.QedfSystem(s.Lx, s.Ltau, s.nrhs, 1 if s.shared_boson else 0)
                                             for s in self.systems])

@@ -60,7 +60,7 @@ def test_every_pcg_candidate_meets_rtol(mode, tmp_path, monkeypatch):
     dev = torch.device("cuda")
     for c in choice["candidates"]:
         s = PcgSolver(systems, mode=mode, rtol=1e-10, max_iter=20000, by=c["by"], slab=c["slab"],
-                      stage=c["stage"], device=dev)
+                      stage=c["stage"], chunk=c["chunk"], device=dev)
         res = s.solve(torch.tensor(phi.reshape(-1), dtype=s.angle_dtype, device=dev),
                       torch.tensor(b.reshape(-1), dtype=s.vec_dtype, device=dev))
         assert res.status.cpu().tolist() == [0] * nrhs, c
