@@ -48,7 +48,7 @@ def parse_args(argv=None):
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--prewarm-seconds", type=float, default=5.0,
+    ap.add_argument("--prewarm-seconds", type=float, default=10.0,
                     help="untimed solver runs on a scratch right-hand side before the warm-up "
                          "trajectories (brings an idle GPU to steady state; the sampler's random "
                          "state is untouched, so the timed trajectories stay the same)")

@@ -257,8 +257,9 @@ typedef struct {
   double rtol;        /* stop when ||b - A x|| / ||b|| <= rtol */
   double dtau;
   int use_precon;     /* builtin tau-banded preconditioner (systems with Ltau >= 26) */
-  int ru_interval;    /* mixed: reliable update at least every ru_interval iterations */
-  double ru_delta;    /* mixed: and whenever the residual fell by this factor */
+  int ru_interval;    /* mixed: reliable update at least every ru_interval iterations
+                         (0 = 100) */
+  double ru_delta;    /* mixed: and whenever the residual fell by this factor (0 = 0.01) */
   int by, slab, chunk;/* tile height (2, 4, 6), tau-slab length of the operator units, sites
                          per elementwise unit (16 or 32); 0 = automatic */
   double timeout_ms;  /* per grid-barrier wait, 0 = 2000 ms */

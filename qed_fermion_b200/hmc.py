@@ -57,7 +57,7 @@ def kernel_to_ref(phi: torch.Tensor, Lx: int, Ltau: int) -> torch.Tensor:
 class HmcSampler:
     def __init__(self, Lx=6, Ltau=10, J=1.0, K=1.0, dtau=0.1, bs=1, delta_t=0.06, N_leapfrog=5, m=1.0,
                  compact=False, precision="mixed", cg_rtol=1e-10, max_iter=20000, use_precon=True,
-                 ru_interval=50, ru_delta=0.1, device=None, seed=None, solver_impl="persistent",
+                 ru_interval=100, ru_delta=0.01, device=None, seed=None, solver_impl="persistent",
                  max_tau_block_idx=1, autotune=True):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {PRECISIONS}")

@@ -81,7 +81,7 @@ class PcgSolver:
 
     def __init__(self, systems: Sequence[System], mode: str = "mixed", rtol: float = 1e-10,
                  max_iter: int = 10000, dtau: float = 0.1, use_precon: bool = True,
-                 ru_interval: int = 50, ru_delta: float = 0.1, by: int = 0, slab: int = 0,
+                 ru_interval: int = 100, ru_delta: float = 0.01, by: int = 0, slab: int = 0,
                  chunk: int = 0, timeout_ms: float = 2000.0, profile: bool = False, device=None,
                  l2_persist: bool = True, stage: bool = False, tune: bool = False):
         if mode not in MODES:
