@@ -167,6 +167,18 @@ int qedf_bb_kspace_acc_c64(const float* A, const float* B, int64_t rows, int Vs,
 int qedf_bb_kspace_acc_c128(const double* A, const double* B, int64_t rows, int Vs, double* S,
                             qedf_stream_t stream);
 
+/* The pair sum of correlator `kind` in one pass: S[k] += sum over the pairs
+ * (ps[p], pt[p]) and all slices of A(k) B(k), A and B the unnormalised 2-D
+ * transforms (e^{+2 pi i k.r / L} and e^{-2 pi i k.r / L}) of the pair's two
+ * fields, which qedf_bb_pair_fields would write; the fields and transforms
+ * stay in shared memory.  Lx must split as p q with q <= 8 and the shared
+ * memory must fit (complex128 up to L = 48, complex64 up to L = 72), else
+ * QEDF_ERR_SIZE: the caller then takes the two-pass path. */
+int qedf_bb_corr_c64(int kind, const float* eta, const float* g_eta, const float* ephase, const int* ps,
+                     const int* pt, int npairs, int Nrv, int Lx, int Ltau, double* S, qedf_stream_t stream);
+int qedf_bb_corr_c128(int kind, const double* eta, const double* g_eta, const double* ephase, const int* ps,
+                      const int* pt, int npairs, int Nrv, int Lx, int Ltau, double* S, qedf_stream_t stream);
+
 /* Tvv (stochastic_estimator.py:1612-1652): writes each noise vector's current
  * field v_s(r) = g_s(r+x) conj(eta_s(r)) e^{i phi_x} + g_s(r) conj(eta_s(r+x))
  * e^{-i phi_x} for all slices ([Nrv][Ltau][Lx*Lx] complex) and adds its sum

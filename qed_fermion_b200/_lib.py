@@ -67,6 +67,8 @@ for _prec in ("c64", "c128"):
     SIGNATURES[f"qedf_bb_pair_fields_{_prec}"] = (
         c_int, [c_int, _vp, _vp, _vp, _vp, _vp, c_int, c_int, c_int, c_int, _vp, _vp, _vp])
     SIGNATURES[f"qedf_bb_kspace_acc_{_prec}"] = (c_int, [_vp, _vp, c_int64, c_int, _vp, _vp])
+    SIGNATURES[f"qedf_bb_corr_{_prec}"] = (
+        c_int, [c_int, _vp, _vp, _vp, _vp, _vp, c_int, c_int, c_int, c_int, _vp, _vp])
     SIGNATURES[f"qedf_bb_vfield_{_prec}"] = (c_int, [_vp, _vp, _vp, c_int, c_int, c_int, _vp, _vp, _vp])
     SIGNATURES[f"qedf_bb_diag_{_prec}"] = (c_int, [_vp, _vp, _vp, c_int, c_int, c_int, _vp, _vp])
 for _r in ("f32", "f64"):

@@ -252,6 +252,225 @@ int diag_entry(const R* eta, const R* g, const R* ep, int Nrv, int Lx, int Ltau,
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
 
+// ----------------------------------------------------------------------------
+// One pass for a whole correlator: per (pair, slice) the two fields, their 2-D
+// transforms and the product, all in shared memory (the fields never reach
+// HBM).  A(k) = sum_r a(r) e^{+2 pi i k.r / L} and B(k) = sum_r b(r)
+// e^{-2 pi i k.r / L} (the unnormalised transforms the two-pass path takes
+// from cuFFT) are formed in place, rows then columns, each line of length
+// L = p q by the two-factor Cooley-Tukey split
+//   X[q k1 + k2] = sum_{n1<p} w_p^{n1 k1} w_L^{n1 k2} sum_{n2<q} x[n1 + p n2] w_q^{n2 k2}
+// (w_m = e^{-+2 pi i / m}); every thread takes whole sub-transforms, with its
+// q (or p) inputs in registers.  Each block adds A(k) B(k) of its items in
+// double precision in shared memory and, at its end, into S.
+// ----------------------------------------------------------------------------
+constexpr int BB_QMAX = 8;  // largest factor of L the kernel is compiled for
+
+// both fields of correlator `kind` for pair (s, t) at site r of slice tau
+template <typename R>
+__device__ __forceinline__ void pair_ab(int kind, const R* eta, const R* g, Cx<R> ep, int64_t os, int64_t ot, int r,
+                                        int r1, Cx<R>& A, Cx<R>& B) {
+  const Cx<R> em = conjc(ep);
+  const Cx<R> ecs = conjc(ldcx(eta, os + r)), ecs1 = conjc(ldcx(eta, os + r1));
+  const Cx<R> gs = ldcx(g, os + r), gs1 = ldcx(g, os + r1);
+  if (kind == 1) {
+    A = cmul(cmul(ecs, ldcx(g, ot + r1)), ep);
+    B = cmul(cmul(gs1, conjc(ldcx(eta, ot + r))), ep);
+  } else if (kind == 4) {
+    A = cmul(cmul(ecs1, ldcx(g, ot + r)), em);
+    B = cmul(cmul(gs, conjc(ldcx(eta, ot + r1))), em);
+  } else {
+    const Cx<R> ect = conjc(ldcx(eta, ot + r)), ect1 = conjc(ldcx(eta, ot + r1));
+    const Cx<R> gt = ldcx(g, ot + r), gt1 = ldcx(g, ot + r1);
+    const R h = (R)0.5;
+    if (kind == 21) {
+      A = h * cmul(cmul(ecs1, gt) + cmul(ect1, gs), em);
+      B = h * cmul(cmul(gs1, ect) + cmul(gt1, ecs), ep);
+    } else {
+      A = h * cmul(cmul(ecs, gt1) + cmul(ect, gs1), ep);
+      B = h * cmul(cmul(gs, ect1) + cmul(gt, ecs1), em);
+    }
+  }
+}
+
+// smem twiddle tables (forward sign e^{-2 pi i ...}); sign +1 uses conjugates
+template <typename R>
+__device__ __forceinline__ Cx<R> tw(const Cx<R>* t, int i, int sgn) {
+  const Cx<R> w = t[i];
+  return sgn > 0 ? conjc(w) : w;
+}
+
+// stage 1 of the transform of `nl` lines of field f (line l, element at
+// base(l) + stride * position): T[line][n1 q + k2] = sum_{n2} x[n1 + p n2] wq^{n2 k2}
+template <typename R>
+__device__ __forceinline__ void dft_stage1(const Cx<R>* X, Cx<R>* T, int L, int p, int q, int line_stride,
+                                           int pos_stride, int item_line, int n1, const Cx<R>* wq, int sgn) {
+  Cx<R> xin[BB_QMAX];
+#pragma unroll
+  for (int n2 = 0; n2 < BB_QMAX; ++n2)
+    if (n2 < q) xin[n2] = X[item_line * line_stride + (n1 + p * n2) * pos_stride];
+  for (int k2 = 0; k2 < q; ++k2) {
+    Cx<R> acc = mk<R>(0, 0);
+#pragma unroll
+    for (int n2 = 0; n2 < BB_QMAX; ++n2)
+      if (n2 < q) acc = cfma(tw(wq, n2 * q + k2, sgn), xin[n2], acc);
+    T[item_line * line_stride + (n1 * q + k2) * pos_stride] = acc;
+  }
+}
+
+// stage 2: X[q k1 + k2] = sum_{n1} wp^{n1 k1} (wL^{n1 k2} T[n1 q + k2])
+template <typename R>
+__device__ __forceinline__ void dft_stage2(Cx<R>* X, const Cx<R>* T, int L, int p, int q, int line_stride,
+                                           int pos_stride, int item_line, int k2, const Cx<R>* wp,
+                                           const Cx<R>* wl, int sgn) {
+  Cx<R> tin[BB_QMAX];
+#pragma unroll
+  for (int n1 = 0; n1 < BB_QMAX; ++n1)
+    if (n1 < p) tin[n1] = cmul(tw(wl, n1 * q + k2, sgn), T[item_line * line_stride + (n1 * q + k2) * pos_stride]);
+  for (int k1 = 0; k1 < p; ++k1) {
+    Cx<R> acc = mk<R>(0, 0);
+#pragma unroll
+    for (int n1 = 0; n1 < BB_QMAX; ++n1)
+      if (n1 < p) acc = cfma(tw(wp, n1 * p + k1, sgn), tin[n1], acc);
+    X[item_line * line_stride + (q * k1 + k2) * pos_stride] = acc;
+  }
+}
+
+template <typename R>
+size_t corr_smem_bytes(int L, int p, int q) {
+  const size_t Vs = (size_t)L * L;
+  return 4 * Vs * sizeof(Cx<R>) + 2 * Vs * sizeof(double) + (size_t)(q * q + p * p + p * q) * sizeof(Cx<R>);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_bb_corr(BondArgs a, int p, int q, double* S) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int L = a.L, Vs = L * L, tid = threadIdx.x, nt = blockDim.x;
+  Cx<R>* F = reinterpret_cast<Cx<R>*>(smraw);  // [2][Vs]: a, b
+  Cx<R>* T = F + 2 * Vs;                        // [2][Vs]: stage temporaries
+  double* P = reinterpret_cast<double*>(T + 2 * Vs);  // [Vs] complex sum
+  Cx<R>* wq = reinterpret_cast<Cx<R>*>(P + 2 * Vs);
+  Cx<R>* wp = wq + q * q;
+  Cx<R>* wl = wp + p * p;
+  for (int i = tid; i < q * q; i += nt) {
+    double sn, cs;
+    sincospi(-2.0 * ((i / q) * (i % q) % q) / q, &sn, &cs);
+    wq[i] = mk<R>((R)cs, (R)sn);
+  }
+  for (int i = tid; i < p * p; i += nt) {
+    double sn, cs;
+    sincospi(-2.0 * ((i / p) * (i % p) % p) / p, &sn, &cs);
+    wp[i] = mk<R>((R)cs, (R)sn);
+  }
+  for (int i = tid; i < p * q; i += nt) {
+    double sn, cs;
+    sincospi(-2.0 * ((i / q) * (i % q) % L) / L, &sn, &cs);
+    wl[i] = mk<R>((R)cs, (R)sn);
+  }
+  for (int i = tid; i < 2 * Vs; i += nt) P[i] = 0.0;
+  __syncthreads();
+  const R* eta = reinterpret_cast<const R*>(a.eta);
+  const R* g = reinterpret_cast<const R*>(a.g);
+  const R* epv = reinterpret_cast<const R*>(a.ep);
+  const int64_t nsite = (int64_t)a.Nt * Vs;
+  const int64_t items = (int64_t)a.npairs * a.Nt;
+  for (int64_t w = blockIdx.x; w < items; w += gridDim.x) {
+    // slice-major order: blocks in flight share their slice's vectors in L2
+    const int tau = (int)(w / a.npairs), pr = (int)(w % a.npairs);
+    const int s = a.ps[pr], t = a.pt[pr];
+    const bool valid = (unsigned)s < (unsigned)a.nrv && (unsigned)t < (unsigned)a.nrv;
+    const int64_t sl = (int64_t)tau * Vs, os = (int64_t)s * nsite + sl, ot = (int64_t)t * nsite + sl;
+    for (int r = tid; r < Vs; r += nt) {
+      const int x = r % L, y = r - x;
+      const int r1 = y + (x + 1 == L ? 0 : x + 1);
+      Cx<R> A = mk<R>(0, 0), B = mk<R>(0, 0);
+      if (valid) pair_ab<R>(a.kind, eta, g, ldcx(epv, sl + r), os, ot, r, r1, A, B);
+      F[r] = A;
+      F[Vs + r] = B;
+    }
+    __syncthreads();
+    // rows (lines y, positions x): A with sign +1, B with sign -1
+    for (int i = tid; i < 2 * L * p; i += nt) {
+      const int f = i / (L * p), rem = i % (L * p);
+      dft_stage1<R>(F + f * Vs, T + f * Vs, L, p, q, L, 1, rem / p, rem % p, wq, f == 0 ? 1 : -1);
+    }
+    __syncthreads();
+    for (int i = tid; i < 2 * L * q; i += nt) {
+      const int f = i / (L * q), rem = i % (L * q);
+      dft_stage2<R>(F + f * Vs, T + f * Vs, L, p, q, L, 1, rem / q, rem % q, wp, wl, f == 0 ? 1 : -1);
+    }
+    __syncthreads();
+    // columns (lines x, positions y); x fastest over the threads
+    for (int i = tid; i < 2 * L * p; i += nt) {
+      const int f = i / (L * p), rem = i % (L * p);
+      dft_stage1<R>(F + f * Vs, T + f * Vs, L, p, q, 1, L, rem % L, rem / L, wq, f == 0 ? 1 : -1);
+    }
+    __syncthreads();
+    for (int i = tid; i < 2 * L * q; i += nt) {
+      const int f = i / (L * q), rem = i % (L * q);
+      dft_stage2<R>(F + f * Vs, T + f * Vs, L, p, q, 1, L, rem % L, rem / L, wp, wl, f == 0 ? 1 : -1);
+    }
+    __syncthreads();
+    for (int k = tid; k < Vs; k += nt) {
+      const Cx<R> u = F[k], v = F[Vs + k];
+      const double ur = u.re, ui = u.im, vr = v.re, vi = v.im;
+      P[2 * k] = fma(ur, vr, fma(-ui, vi, P[2 * k]));
+      P[2 * k + 1] = fma(ur, vi, fma(ui, vr, P[2 * k + 1]));
+    }
+    __syncthreads();
+  }
+  for (int k = tid; k < Vs; k += nt) {
+    atomicAdd(S + 2 * k, P[2 * k]);
+    atomicAdd(S + 2 * k + 1, P[2 * k + 1]);
+  }
+}
+
+// the factor split L = p q with q <= BB_QMAX and p as large as possible (p <= q)
+inline bool corr_factors(int L, int& p, int& q) {
+  p = 0;
+  for (int d = 1; d * d <= L; ++d)
+    if (L % d == 0 && L / d <= BB_QMAX) p = d;
+  if (!p) return false;
+  q = L / p;
+  return true;
+}
+
+template <typename R>
+int corr_entry(int kind, const R* eta, const R* g, const R* ep, const int* ps, const int* pt, int npairs, int Nrv,
+               int Lx, int Ltau, double* S, cudaStream_t st) {
+  if (kind != 1 && kind != 21 && kind != 2 && kind != 4) return QEDF_ERR_ARG;
+  if (!eta || !g || !ep || !ps || !pt || !S) return QEDF_ERR_ARG;
+  if (npairs < 0 || Lx < 2 || Ltau < 1 || Nrv < 2) return QEDF_ERR_ARG;
+  int p, q;
+  if (!corr_factors(Lx, p, q)) return QEDF_ERR_SIZE;
+  const size_t smem = corr_smem_bytes<R>(Lx, p, q);
+  if (smem > 227 * 1024) return QEDF_ERR_SIZE;
+  if (npairs == 0) return QEDF_OK;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(k_bb_corr<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return QEDF_ERR_CUDA;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bb_corr<R>, 256, smem) != cudaSuccess || per_sm < 1)
+    return QEDF_ERR_SIZE;
+  BondArgs a;
+  a.kind = kind;
+  a.eta = eta;
+  a.g = g;
+  a.ep = ep;
+  a.ps = ps;
+  a.pt = pt;
+  a.npairs = npairs;
+  a.nrv = Nrv;
+  a.L = Lx;
+  a.Nt = Ltau;
+  a.fa = nullptr;
+  a.fb = nullptr;
+  const int64_t items = (int64_t)npairs * Ltau;
+  const int blocks = (int)std::min<int64_t>(items, (int64_t)num_sms() * per_sm);
+  k_bb_corr<R><<<blocks, 256, smem, st>>>(a, p, q, S);
+  return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
+}
+
 template <typename R>
 int pair_fields_entry(int kind, const R* eta, const R* g, const R* ep, const int* ps, const int* pt, int npairs,
                       int Nrv, int Lx, int Ltau, R* fa, R* fb, cudaStream_t st) {
@@ -313,6 +532,16 @@ int qedf_bb_kspace_acc_c64(const float* A, const float* B, int64_t rows, int Vs,
 int qedf_bb_kspace_acc_c128(const double* A, const double* B, int64_t rows, int Vs, double* S,
                             qedf_stream_t s) {
   return kspace_acc_entry<double>(A, B, rows, Vs, S, reinterpret_cast<cudaStream_t>(s));
+}
+int qedf_bb_corr_c64(int kind, const float* eta, const float* g_eta, const float* ephase, const int* ps,
+                     const int* pt, int npairs, int Nrv, int Lx, int Ltau, double* S, qedf_stream_t s) {
+  return corr_entry<float>(kind, eta, g_eta, ephase, ps, pt, npairs, Nrv, Lx, Ltau, S,
+                           reinterpret_cast<cudaStream_t>(s));
+}
+int qedf_bb_corr_c128(int kind, const double* eta, const double* g_eta, const double* ephase, const int* ps,
+                      const int* pt, int npairs, int Nrv, int Lx, int Ltau, double* S, qedf_stream_t s) {
+  return corr_entry<double>(kind, eta, g_eta, ephase, ps, pt, npairs, Nrv, Lx, Ltau, S,
+                            reinterpret_cast<cudaStream_t>(s));
 }
 int qedf_bb_vfield_c64(const float* eta, const float* g_eta, const float* ephase, int Nrv, int Lx, int Ltau,
                        float* v, double* Tv, qedf_stream_t s) {

@@ -29,10 +29,13 @@ from . import ops
 
 
 class BondBond:
-    def __init__(self, Lx: int, Ltau: int, chunk_bytes: int = 1 << 30):
+    def __init__(self, Lx: int, Ltau: int, chunk_bytes: int = 1 << 30, fused: bool = True):
         self.Lx = self.Ly = Lx
         self.Ltau = Ltau
         self.chunk_bytes = int(chunk_bytes)
+        # one-pass pair sums (ops.bb_corr) where the lattice fits that kernel;
+        # fused=False takes the two-pass path (pair fields, cuFFT, k-space sum)
+        self.fused = bool(fused)
 
     # ---- helpers ----------------------------------------------------------
     def _chunk(self, ec, n_arrays=4):
@@ -52,10 +55,13 @@ class BondBond:
         ep = torch.exp(1j * ph).to(dt).contiguous()
         Vs = self.Lx * self.Ly
         pairs = torch.combinations(torch.arange(nrv, device=e.device), r=2, with_replacement=False).to(torch.int32)
+        S = torch.zeros(Vs, dtype=torch.complex128, device=e.device)
+        if self.fused and ops.bb_corr(kind, e, g, ep, pairs[:, 0].contiguous(), pairs[:, 1].contiguous(), self.Lx, S):
+            S = S.view(self.Ly, self.Lx) / (Vs * Vs)
+            return (torch.fft.ifft2(S, norm="forward") / (len(pairs) * self.Ltau)).to(dt)
         chunk = min(65535, self._chunk(e.reshape(nrv, self.Ltau, self.Ly, self.Lx)), len(pairs))
         fa = torch.empty((chunk, self.Ltau, self.Ly, self.Lx), dtype=dt, device=e.device)
         fb = torch.empty_like(fa)
-        S = torch.zeros(Vs, dtype=torch.complex128, device=e.device)
         for ch in pairs.split(chunk):
             n = len(ch)
             a, b = fa[:n], fb[:n]

@@ -179,6 +179,28 @@ def bb_pair_fields(kind: str, eta: torch.Tensor, g_eta: torch.Tensor, ephase: to
               npairs, nrv, Lx, Ltau, ptr(fa), ptr(fb), stream_handle())
 
 
+def bb_corr(kind: str, eta: torch.Tensor, g_eta: torch.Tensor, ephase: torch.Tensor, ps: torch.Tensor,
+            pt: torch.Tensor, Lx: int, S: torch.Tensor) -> bool:
+    """S[k] += the pair sum of correlator ``kind`` over the pairs (ps, pt) and
+    all slices in one pass (fields and transforms in shared memory).  Returns
+    False without launching when the lattice does not fit the fused kernel
+    (the caller then takes ``bb_pair_fields`` + FFTs + ``bb_kspace_acc``)."""
+    prec, nrv, N, Vs, Ltau = _bb_inputs("bb_corr", eta, g_eta, ephase, Lx)
+    _check_cuda(ps, pt, S)
+    if ps.dtype != torch.int32 or pt.dtype != torch.int32 or not ps.is_contiguous() or not pt.is_contiguous():
+        raise RuntimeError("bb_corr: pair indices must be contiguous int32")
+    if S.dtype != torch.complex128 or S.numel() != Vs or not S.is_contiguous() or pt.numel() != ps.numel():
+        raise RuntimeError("bb_corr: S must be a contiguous complex128 buffer of Lx^2 entries")
+    st = getattr(_lib.load(), f"qedf_bb_corr_{prec}")(BB_KINDS[kind], ptr(eta), ptr(g_eta), ptr(ephase), ptr(ps), ptr(pt),
+                                            ps.numel(), nrv, Lx, Ltau, ptr(S), stream_handle())
+    if st == _lib.QEDF_ERR_SIZE:
+        return False
+    if st != _lib.QEDF_OK:
+        raise _lib.QedfError("qedf_bb_corr", st, _lib.status_string(st))
+    _lib.LAUNCHES["count"] += 1
+    return True
+
+
 def bb_kspace_acc(A: torch.Tensor, B: torch.Tensor, S: torch.Tensor) -> None:
     """S[k] += sum over rows of A[..., k] B[..., k] (the last two dimensions of
     A, B are the spatial modes), accumulated in double precision into the
