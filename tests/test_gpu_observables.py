@@ -136,3 +136,22 @@ def test_t2_is_t21_reflected(cdt, tol):
     bb = BondBond(L, Nt)
     want = bb.T2_direct(eta, g, bos)
     assert rel(bb.T2(eta, g, bos).cpu(), want.cpu()) < tol
+
+
+@pytest.mark.parametrize("L,Lt,nrv,cdt,tol", [(12, 20, 6, torch.complex128, 1e-12), (18, 8, 5, torch.complex128, 1e-12),
+                                             (36, 6, 4, torch.complex64, 2e-5), (10, 12, 4, torch.complex128, 1e-12),
+                                             (34, 4, 3, torch.complex128, 1e-12)])
+def test_fused_pair_sums_match_two_pass(L, Lt, nrv, cdt, tol):
+    """The one-pass correlator kernel (fields, transforms and k-space product in
+    shared memory) against the two-pass path (pair fields, cuFFT, k-space sum);
+    L = 34 = 2 x 17 does not split into factors <= 8 and takes the two-pass path."""
+    from qed_fermion_b200.observables import BondBond
+    g = torch.Generator(device=DEV).manual_seed(L + Lt)
+    N = L * L * Lt
+    eta = torch.randn((nrv, N), dtype=cdt, device=DEV, generator=g)
+    G = torch.randn((nrv, N), dtype=cdt, device=DEV, generator=g)
+    bos = torch.rand((1, 2, L, L, Lt), dtype=torch.float64, device=DEV, generator=g) * 6.28
+    for name in ("T1", "T21", "T2_direct", "T4"):
+        a = getattr(BondBond(L, Lt, fused=True), name)(eta, G, bos)
+        b = getattr(BondBond(L, Lt, fused=False), name)(eta, G, bos)
+        assert float((a - b).abs().max() / b.abs().max()) < tol, name
