@@ -856,7 +856,12 @@ def run_configs(args):
           "iters": int(se.iters.max()), "relres": float(se.relres.max()), "tuned": tuned(se.solver)})
     ms, _ = timed(lambda: se.get_bond_bond_per_b2(bos))
     emit({"config": "C4a", "what": "bond-bond correlators T1+T21+T2+T4+Tvv over the 2016 noise pairs "
-                                   "(complex128, cuFFT)", "ms": ms})
+                                   "(complex128, pair-field and k-space kernels around cuFFT)", "ms": ms})
+    se.corr_dtype = torch.complex64
+    ms, _ = timed(lambda: se.get_bond_bond_per_b2(bos))
+    emit({"config": "C4a", "what": "the same correlators in complex64 (the reference estimator's precision)",
+          "ms": ms})
+    se.corr_dtype = None
     # where one correlator's time goes: the passes of one chunk of pairs (the
     # default 1 GiB chunk: 34 pairs), each timed over 10 launches
     e128 = se.eta.to(torch.complex128).resolve_conj().contiguous()

@@ -20,7 +20,7 @@ from .solver import PcgSolver, System
 
 class StochaticEstimator:
     def __init__(self, Lx, Ltau, Nrv=20, dtau=0.1, precision="mixed", cg_rtol=1e-10, max_iter=20000,
-                 use_precon=True, device=None, seed=None, noise="z2z2", autotune=True):
+                 use_precon=True, device=None, seed=None, noise="z2z2", autotune=True, corr_dtype=None):
         self.Lx, self.Ly, self.Ltau, self.Nrv, self.dtau = Lx, Lx, Ltau, Nrv, dtau
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         self.noise = noise
@@ -33,6 +33,10 @@ class StochaticEstimator:
                                 tune=autotune)
         self.eta = None
         self.G_eta = None
+        # complex dtype of the bond-bond correlators' arithmetic: None keeps
+        # that of eta / G_eta; torch.complex64 is the reference estimator's
+        # own precision and halves their memory traffic
+        self.corr_dtype = corr_dtype
 
     def random_vec_bin(self):
         """Nrv vectors with entries (+-1 +- i)/sqrt(2) (reference :210-224); with
@@ -78,8 +82,12 @@ class StochaticEstimator:
         return self._bb().Tvv(eta, G_eta, boson)
 
     def get_bond_bond_per_b2(self, boson):
-        """The observables of the current eta / G_eta (after set_eta_G_eta)."""
-        return self._bb().get_bond_bond_per_b2(self.eta, self.G_eta, boson)
+        """The observables of the current eta / G_eta (after set_eta_G_eta), in
+        ``corr_dtype`` when it is set."""
+        eta, g = self.eta, self.G_eta
+        if self.corr_dtype is not None:
+            eta, g = eta.to(self.corr_dtype), g.to(self.corr_dtype)
+        return self._bb().get_bond_bond_per_b2(eta, g, boson)
 
     def bond_corr(self, BB_r_mean, B_r_mean):
         return self._bb().bond_corr(BB_r_mean, B_r_mean)
