@@ -62,6 +62,10 @@ def parse_args(argv=None):
     ap.add_argument("--fp64-steps", type=int, default=5, help="trajectories timed on the plain FP64 path")
     ap.add_argument("--bf16-steps", type=int, default=5,
                     help="trajectories timed with the PCG's vectors stored as bf16 (mixed arithmetic)")
+    ap.add_argument("--graph-steps", type=int, default=10,
+                    help="trajectories timed with each trajectory replayed from a CUDA graph (mixed)")
+    ap.add_argument("--chrono-steps", type=int, default=10,
+                    help="trajectories timed with the leapfrog's solves started from extrapolated solutions")
     ap.add_argument("--dropin-steps", type=int, default=1,
                     help="trajectories of the reference's per-iteration loop on the _C kernels (complex128)")
     ap.add_argument("--accept-steps", type=int, default=20,
@@ -346,10 +350,11 @@ def run_native(args):
     seed = replica_seed(args.seed, rank)
     rng = np.random.default_rng(seed)
 
-    def make(precision, solver_impl="persistent"):
+    def make(precision, solver_impl="persistent", graph=False, chrono_guess=None):
         h = HmcSampler(Lx=L, Ltau=Lt, J=1.0, K=1.0, dtau=0.1, bs=bs, delta_t=args.delta_t,
                        N_leapfrog=args.n_leapfrog, precision=precision, cg_rtol=args.rtol, max_iter=20000,
-                       device=dev, seed=seed, solver_impl=solver_impl, autotune=args.autotune)
+                       device=dev, seed=seed, solver_impl=solver_impl, autotune=args.autotune, graph=graph,
+                       chrono_guess=chrono_guess)
         return h
 
     hmc = make("mixed")
@@ -485,8 +490,9 @@ def run_native(args):
         e1.record(stream)
         torch.cuda.synchronize()
         t = e0.elapsed_time(e1) / 1e3
+        shape = ({k: h.solver.tuned[k] for k in ("by", "slab", "stage", "chunk")} if h.solver.tuned else None)
         return {"value": 3600.0 * n * bs / t, "unit": UNIT, "steps": n, "s_per_trajectory": t / n,
-                "cg_iters_per_solve": float(torch.stack(its).double().mean())}
+                "cg_iters_per_solve": float(torch.stack(its).double().mean()), "pcg_launch_shape": shape}
 
     # --- plain FP64 path, same workload
     fp64 = None
@@ -505,6 +511,27 @@ def run_native(args):
             fp64["dropin"]["path"] = ("reference loop structure (preconditioned_cg_fast_test) on _C kernels, "
                                       "complex128")
             del hd
+
+    # --- the same trajectories replayed from a CUDA graph (one graph launch per
+    # trajectory; the first proposal, in the warm-up, captures it)
+    graph = None
+    if rank == 0 and args.graph_steps > 0 and not args.quick:
+        hg = make("mixed", graph=True)
+        hg.boson = hmc.boson.clone()
+        graph = time_trajectories(hg, args.graph_steps)
+        graph["path"] = "mixed precision, each trajectory replayed from a CUDA graph"
+        del hg
+
+    # --- the leapfrog's solves started from the linear extrapolation of the
+    # previous two solutions instead of zero
+    chrono = None
+    if rank == 0 and args.chrono_steps > 0 and not args.quick:
+        hc = make("mixed", chrono_guess="linear")
+        hc.boson = hmc.boson.clone()
+        chrono = time_trajectories(hc, args.chrono_steps)
+        chrono["path"] = ("mixed precision; each leapfrog solve after the first starts from the linear "
+                          "extrapolation of the previous two solutions (the reference starts from zero)")
+        del hc
 
     # --- bf16 vector storage, same workload
     bf16 = None
@@ -531,7 +558,8 @@ def run_native(args):
         del h64
         dHd = (H1d - H0d).cpu()
         dH = {"dH_fp64": dHd.tolist(), "H0": H0d.cpu().tolist()}
-        for name, h in (("mixed", hmc), ("mixed_bf16", make("mixed_bf16"))):
+        for name, h in (("mixed", hmc), ("mixed_bf16", make("mixed_bf16")),
+                        ("mixed_chrono_linear", make("mixed", chrono_guess="linear"))):
             _, H0m, H1m, _, _ = h.leapfrog_proposer5(x0.to(torch.float32), p0=p0.to(torch.float32), R=R)
             dHm = (H1m - H0m).cpu()
             dH[name] = {"dH": dHm.tolist(), "abs_err": (dHm - dHd).abs().tolist(),
@@ -635,7 +663,7 @@ def run_native(args):
                                        if fp64 and "dropin" in fp64 else None),
             "pcg_launch_shape": ({k: hmc.solver.tuned[k] for k in ("by", "slab", "stage", "chunk")}
                                  if hmc.solver.tuned else None),
-            "bf16": bf16, "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate,
+            "bf16": bf16, "graph": graph, "chrono": chrono, "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate,
             "acceptance_vs_fp64": acc, **result,
         }
         print(json.dumps(line), flush=True)

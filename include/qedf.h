@@ -287,6 +287,10 @@ typedef struct {
   int stage;          /* 1: the operator passes stage their input slices in shared memory by
                          bulk copies where the stages fit (single-precision iterations);
                          0 (default) or -1: the engine that loads them directly */
+  int x_init;         /* 1: x holds an initial guess on entry; the solve starts from the
+                         residual b - A x, computed in the high precision (double for
+                         MIXED / MIXED_BF16 / PLAIN_F64).  A right-hand side with b = 0
+                         gets x = 0.  0 (default): x starts at 0, as in the reference */
 } qedf_pcg_opts;
 
 /* Bytes of device workspace qedf_pcg_solve needs for these systems. */

@@ -48,6 +48,7 @@ class QedfPcgOpts(ctypes.Structure):
         ("profile", c_void_p),
         ("l2_persist", c_int),
         ("stage", c_int),
+        ("x_init", c_int),
     ]
 
 

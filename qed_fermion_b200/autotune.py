@@ -12,9 +12,11 @@ device once per problem shape and remembered:
   them directly, and 16- or 32-site elementwise units.
 * M^dag M (``qedf_mhm_vec_*``): tile height and slab length.
 
-Each candidate runs a short fixed-iteration solve (or a few operator
-applications) on seeded synthetic inputs of the same shape, timed with CUDA
-events after a warm-up; the fastest wins.  Every candidate computes the same
+Each candidate runs a fixed-iteration solve of 100 iterations (or an
+operator application) on seeded synthetic inputs of the same shape, timed
+with CUDA events: the fastest of a few calls after an untimed one, all after
+about a second of solves that bring the GPU's clocks up.  The fastest
+candidate wins.  Every candidate computes the same
 iteration (tests check each against the oracle), so the choice only changes
 the time.  Results are kept in memory and in a JSON file (``QEDF_TUNE_CACHE``,
 default ``~/.cache/qed_fermion_b200/tune.json``), keyed by the device, the
@@ -26,6 +28,7 @@ import json
 import math
 import os
 import threading
+import time
 
 import torch
 
@@ -106,15 +109,30 @@ def _remember(key, value):
 
 
 def _time(fn, reps):
+    """Milliseconds of one call: the fastest of ``reps`` calls timed one by
+    one with CUDA events, after one untimed call."""
     fn()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
+    best = None
     for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         fn()
-    e1.record()
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1) / reps
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    return best
+
+
+def _warm_gpu(fn, seconds):
+    """Run ``fn`` for about ``seconds`` of wall time, so that the candidates
+    timed next see the clocks of a busy GPU rather than those of an idle one
+    (the first candidate of a cold process otherwise reads up to 10x slow)."""
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        fn()
+        torch.cuda.synchronize()
 
 
 def _synthetic(systems, angle_dtype, vec_dtype, device, seed=20261204):
@@ -135,7 +153,7 @@ def _synthetic(systems, angle_dtype, vec_dtype, device, seed=20261204):
     return torch.cat(phis).to(angle_dtype), torch.cat(bs).to(vec_dtype)
 
 
-def pcg_choice(systems, mode, use_precon=True, dtau=0.1, iters=30, force=False) -> dict:
+def pcg_choice(systems, mode, use_precon=True, dtau=0.1, iters=100, force=False, warm_seconds=1.0) -> dict:
     """The fastest (by, slab, stage) for this batch of systems and precision
     mode, timed once and then cached.  Returns a dict with the choice, its
     microseconds per iteration and the timings of every candidate."""
@@ -162,8 +180,13 @@ def pcg_choice(systems, mode, use_precon=True, dtau=0.1, iters=30, force=False) 
             continue
         if phi is None:
             phi, b = _synthetic(systems, s.angle_dtype, s.vec_dtype, device)
+            try:
+                _warm_gpu(lambda: s.solve(phi, b), warm_seconds)
+            except _lib.QedfError:
+                phi = None
+                continue
         try:
-            ms = _time(lambda: s.solve(phi, b), reps=2)
+            ms = _time(lambda: s.solve(phi, b), reps=3)
         except _lib.QedfError:
             continue  # a shape this launch cannot take (shared memory, threads)
         timings.append({"by": by, "slab": T, "stage": st, "chunk": ch, "us_per_iter": 1e3 * ms / iters})

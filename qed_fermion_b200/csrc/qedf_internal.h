@@ -112,6 +112,7 @@ struct PcgParams {
   int xs;    // allow the warp-shuffle engine for the single-precision iterations
   int stage; // 1: allow the staged operator engine (EC_STAGE) where its shared memory fits
   int stage_off;  // bytes: start of the operator passes' slice stages in dynamic shared memory
+  int x_init;     // 1: x holds an initial guess on entry (the solve starts from b - A x)
   int l2;    // 0: L2 persisting window over the iteration vectors when they fit; -1: off
   int max_iter, ru_interval;
   double rtol, ru_delta;

@@ -278,14 +278,17 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     c0 = (lu % S.nchunk) * CH;
     c1 = min(c0 + CH, Vs);
   };
+  // plain modes with an initial guess: the first pass forms r = b - A x (below)
+  bool guess_pass = false;
   auto vec_base = [&](int s, int v) -> int64_t {
     const PcgSys& S = p.sys[s];
     return S.vec0 + (int64_t)(v - S.rhs0) * S.Nt * SL(S) * SL(S);
   };
 
   // ---- BC-type elementwise pass over one unit --------------------------------
-  // kind 0: init (x = 0, r = b, bb); 1: iteration update; 2: preconditioner only
-  // (after a reliable update).  A unit is CHC sites of one right-hand side over
+  // kind 0: init (x = 0 unless it holds an initial guess, r = b, bb); 1:
+  // iteration update; 2: preconditioner only (after a reliable update or the
+  // initial guess's residual).  A unit is CHC sites of one right-hand side over
   // all tau; a thread handles two neighbouring sites (one 16-byte access per
   // vector in single precision) in every (blockDim/PPR)-th row.  r of the unit
   // stays in shared memory for the tau-stencil of the preconditioner, whose
@@ -356,8 +359,9 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         acc_a += (double)b0.re * b0.re + (double)b0.im * b0.im + (double)b1.re * b1.re + (double)b1.im * b1.im;
         r0 = mk<RS>((RS)b0.re, (RS)b0.im);
         r1 = mk<RS>((RS)b1.re, (RS)b1.im);
-        st2s(xs + i2, mk<RS>(0, 0), mk<RS>(0, 0));
-        if (MIXED) st2(xh + i2, mk<RH>(0, 0), mk<RH>(0, 0));
+        // x_lo (mixed) always starts at 0; x itself unless it is the guess
+        if (MIXED || !p.x_init) st2s(xs + i2, mk<RS>(0, 0), mk<RS>(0, 0));
+        if (MIXED && !p.x_init) st2(xh + i2, mk<RH>(0, 0), mk<RH>(0, 0));
         st2s(r + i2, r0, r1);
       } else if (kind == 1) {
         Cx<RS> o0, o1;
@@ -466,7 +470,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     RS* xl = xs + vb;
     const SP* pold = reinterpret_cast<const SP*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
     SP* pnew = reinterpret_cast<SP*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
-    const SP* zz = ((S.precon || BF) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
+    const SP* zz = (guess_pass ? reinterpret_cast<const SP*>(xs)
+                               : (S.precon || BF) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
     RS* O = Op + vb;
     const RS t1 = (RS)p.t1, th = (RS)p.th, Cb = (RS)p.Cb;
     Cx<RS> X0[BY][2], X1[BY][2], Y[BY][2];
@@ -577,7 +582,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     RS* xl = xs + vb;
     const SP* pold = reinterpret_cast<const SP*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
     SP* pnew = reinterpret_cast<SP*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
-    const SP* zz = ((S.precon || BF) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
+    const SP* zz = (guess_pass ? reinterpret_cast<const SP*>(xs)
+                               : (S.precon || BF) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
     RS* O = Op + vb;
     const RS t1 = (RS)p.t1, th = (RS)p.th, Cb = (RS)p.Cb;
     // slots of the iteration precision; z and p_old may be narrower
@@ -788,6 +794,23 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     }
   };
 
+  // x = 0 for a right-hand side with b = 0 (its guess is replaced by the
+  // exact solution)
+  auto zero_x_unit = [&](int u) {
+    int s, v, c0, c1;
+    unitE(u, s, v, c0, c1);
+    if (acc.bb[v] != 0.0) return;
+    const PcgSys& S = p.sys[s];
+    const int Vs = SL(S) * SL(S), w = c1 - c0;
+    const int64_t base = vec_base(s, v);
+    const int j = tid % PPR;
+    if (2 * j >= w) return;
+    for (int t = tid / PPR; t < S.Nt; t += blockDim.x / PPR) {
+      const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
+      st2(xh + i2, mk<RH>(0, 0), mk<RH>(0, 0));
+    }
+  };
+
   // plain modes, end of the solve: x += alpha p_last where still pending
   auto flush_unit = [&](int u) {
     int s, v, c0, c1;
@@ -817,7 +840,6 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   // init: x = 0, r = b, z = P r
   for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) elementwise(0, u, 0);
   ok = grid_barrier(p.bar, nblk, budget, bar_target);
-  pc.lap(0);
   int slot = 0;  // accumulator slot holding the current rr / rz
   if (ok) {
     for (int v = tid; v < NV; v += blockDim.x) {
@@ -832,6 +854,16 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     }
     __syncthreads();
   }
+  // initial guess: a right-hand side with b = 0 gets x = 0.  Mixed modes start
+  // the others with a reliable update (r = b - A x in double, z = P r); plain
+  // modes with one pass of the iteration's own two phases on p = x (guess
+  // pass: Op = A x, then r = b - 1 * Op and z = P r), which counts no
+  // iteration and updates no x
+  if (ok && p.x_init) {
+    for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) zero_x_unit(u);
+    guess_pass = !MIXED;
+  }
+  pc.lap(0);
 
   int it = 0;
   while (ok) {
@@ -853,7 +885,9 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         continue;
       }
       if (MIXED) {
-        if (res <= p.rtol || it - st.lastru[v] >= p.ru_interval || res < p.ru_delta * st.resmax[v]) {
+        // (the initial guess's residual is a reliable update's)
+        if (res <= p.rtol || it - st.lastru[v] >= p.ru_interval || res < p.ru_delta * st.resmax[v] ||
+            (it == 0 && p.x_init)) {
           st.ru[v] = 1;
           st.any_ru = 1;
         }
@@ -910,7 +944,9 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     // ---- phase A
     for (int v = tid; v < NV; v += blockDim.x) st.beta[v] = st.iters[v] > 0 ? st.rz[v] / st.rzold[v] : 0.0;
     __syncthreads();
-    const int aslot = it & 1;
+    // (the guess pass uses the pAp slot of odd iterations, so that its BC
+    // phase clears the slot of iteration 0)
+    const int aslot = guess_pass ? 1 : it & 1;
     for (int u = blockIdx.x; u < p.unitsA; u += gridDim.x) {
       const int s = find_sys_A(p, u);
       const int v = p.sys[s].rhs0 + (u - p.sys[s].unitA0) / p.sys[s].nslab;
@@ -933,7 +969,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     // alpha of inactive systems stays that of their last iteration: a pending
     // x update still uses it
     for (int v = tid; v < NV; v += blockDim.x)
-      if (st.active[v]) st.alpha[v] = st.rz[v] / acc.pAp[aslot * NV + v];
+      if (st.active[v]) st.alpha[v] = guess_pass ? 1.0 : st.rz[v] / acc.pAp[aslot * NV + v];
     __syncthreads();
     for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) {
       int s, v, c0, c1;
@@ -951,11 +987,13 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       st.rzold[v] = st.rz[v];
       st.rz[v] = acc.rz[slot * NV + v];
       st.rr[v] = acc.rr[slot * NV + v];
+      if (guess_pass) continue;
       st.iters[v] += 1;
       st.pending[v] = 1;
     }
     __syncthreads();
-    ++it;
+    if (guess_pass) guess_pass = false;
+    else ++it;
     pc.lap(6);
   }
   if (pc.prof) {
@@ -1026,6 +1064,7 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
   p.nsys = nsys;
   p.xs = 1;
   p.stage = o->stage > 0 ? 1 : 0;
+  p.x_init = o->x_init > 0 ? 1 : 0;
   p.l2 = o->l2_persist < 0 ? -1 : 0;
   if (o->chunk != 0 && o->chunk != 16 && o->chunk != 32) return QEDF_ERR_ARG;
   // 32-site elementwise units (one longer tau column per block) fit where

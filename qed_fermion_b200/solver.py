@@ -107,6 +107,9 @@ class PcgSolver:
                                       int(slab), int(chunk), float(timeout_ms),
                                       self.profile.data_ptr() if profile else None,
                                       0 if l2_persist else -1, 1 if stage else 0)
+        # the same options with x holding an initial guess on entry
+        self._opts_x0 = _lib.QedfPcgOpts.from_buffer_copy(self._opts)
+        self._opts_x0.x_init = 1
         nbytes = _lib.load().qedf_pcg_workspace_bytes(self._sys, n, self._opts)
         if nbytes < 0:
             raise ValueError("invalid system description for the PCG solver")
@@ -117,9 +120,12 @@ class PcgSolver:
         self.vec_dtype = VEC_DTYPE[mode]
         self.angle_dtype = ANGLE_DTYPE[mode]
 
-    def solve(self, boson: torch.Tensor, b: torch.Tensor, out: SolveResult = None) -> SolveResult:
+    def solve(self, boson: torch.Tensor, b: torch.Tensor, out: SolveResult = None,
+              x0: torch.Tensor = None) -> SolveResult:
         """``boson``: packed angles; ``b``: packed right-hand sides (any shape
-        with the right number of elements)."""
+        with the right number of elements).  ``x0``: an optional initial guess
+        like ``b``; the solve then starts from the residual ``b - A x0``,
+        computed in the high precision (the reference starts from 0)."""
         if boson.dtype != self.angle_dtype or boson.numel() != self.angle_len:
             raise RuntimeError(f"boson must hold {self.angle_len} {self.angle_dtype} angles")
         if b.dtype != self.vec_dtype or b.numel() != self.vec_len:
@@ -133,9 +139,16 @@ class PcgSolver:
                               torch.empty(self.nrhs, dtype=torch.int32, device=b.device),
                               torch.empty(self.nrhs, dtype=torch.float64, device=b.device),
                               torch.empty(self.nrhs, dtype=torch.int32, device=b.device))
+        opts = self._opts
+        if x0 is not None:
+            if x0.dtype != self.vec_dtype or x0.numel() != self.vec_len:
+                raise RuntimeError(f"x0 must hold {self.vec_len} {self.vec_dtype} entries")
+            if x0.data_ptr() != out.x.data_ptr():
+                out.x.copy_(x0.reshape(out.x.shape))
+            opts = self._opts_x0
         _lib.call("qedf_pcg_solve", self._sys, len(self.systems), ptr(boson), ptr(b), ptr(out.x),
                   ptr(out.iters), ptr(out.relres), ptr(out.status), ptr(self.workspace),
-                  self.workspace.numel(), self._opts, stream_handle())
+                  self.workspace.numel(), opts, stream_handle())
         return out
 
 

@@ -89,3 +89,44 @@ def test_operator_replays_in_cuda_graph():
     torch.cuda.synchronize()
     want = ops.apply_operator("mhm", phi1.float().view(bs, -1), x1.to(torch.complex64).view(bs, -1), L, 0.1)
     assert torch.equal(out, want)
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_trajectory_graph_matches_eager(precision):
+    """Metropolis updates with the trajectory replayed from a CUDA graph give
+    the eager sampler's fields, Hamiltonians and decisions: same seed, so the
+    same draws; the first proposal runs eagerly and captures, the later ones
+    replay.  Tau-block proposals use their own (masked) graph."""
+    from qed_fermion_b200 import _lib
+    from qed_fermion_b200.hmc import HmcSampler
+    dev = torch.device("cuda:0")
+    kw = dict(Lx=6, Ltau=60, bs=2, delta_t=0.02, N_leapfrog=3, precision=precision, cg_rtol=1e-10,
+              device=dev, seed=7, max_tau_block_idx=1, autotune=False)
+    runs = {}
+    for graph in (False, True):
+        h = HmcSampler(graph=graph, **kw)
+        h.initialize_boson_pi_flux_randn_matfree()
+        out = []
+        for _ in range(3):
+            n0 = _lib.LAUNCHES["count"]
+            boson, accp, it, err, H0, H1 = h.metropolis_update()
+            out.append((boson.clone(), accp.clone(), H0.clone(), H1.clone(), it.clone(), _lib.LAUNCHES["count"] - n0))
+        mask = torch.zeros((1, 1, 1, 1, h.Ltau), device=dev, dtype=h.dtype)
+        mask[..., :20] = 1.0
+        for _ in range(2):
+            boson, accp, it, err, H0, H1 = h.metropolis_update(tau_mask=mask)
+            out.append((boson.clone(), accp.clone(), H0.clone(), H1.clone(), it.clone(), 0))
+        torch.cuda.synchronize()
+        runs[graph] = (out, [list(q) for q in h.threshold_queue], h)
+    (e, qe, he), (g, qg, hg) = runs[False], runs[True]
+    assert len(hg._graphs) == 2 and all(tg.graph is not None for tg in hg._graphs.values())
+    for (b0, a0, h00, h10, i0, n0), (b1, a1, h01, h11, i1, n1) in zip(e, g):
+        assert torch.equal(a0, a1)
+        assert torch.allclose(h00, h01, rtol=1e-12, atol=0) and torch.allclose(h10, h11, rtol=1e-12, atol=0)
+        assert torch.allclose(b0, b1, rtol=0, atol=1e-9 if precision == "fp64" else 1e-5)
+        assert torch.all((i0 - i1).abs() <= 1)
+    # the launch counter sees the replays' kernels
+    assert [o[5] for o in g[:3]] == [o[5] for o in e[:3]]
+    assert len(qe) == len(qg)
+    for a, b in zip(qe, qg):
+        assert a == pytest.approx(b, rel=1e-9, abs=1e-12)

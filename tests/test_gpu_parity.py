@@ -343,6 +343,70 @@ def test_pcg_truncated_solves_match_oracle_iterates(mode, tol, iters):
     assert relerr(res.x.cpu().numpy().reshape(bs, -1), xo) < tol
 
 
+@pytest.mark.parametrize("mode,tol", [("fp64", 1e-11), ("mixed", 2e-5), ("fp32", 2e-5)])
+@pytest.mark.parametrize("iters", [1, 5])
+def test_pcg_initial_guess_iterates_match_oracle(mode, tol, iters):
+    """PCG from an initial guess x0 is x0 plus PCG from zero on the residual
+    b - A x0: truncated solves against the oracle's iterates of that shifted
+    system."""
+    from qed_fermion_b200.solver import PcgSolver, System
+    L, Nt, bs = 4, 30, 2
+    boson, b = rand_case(L, Nt, bs, seed=78, kind="piflux")
+    rng = np.random.default_rng(5)
+    x0 = (rng.standard_normal(b.shape) + 1j * rng.standard_normal(b.shape)) * 0.3
+    phi = O.ref_to_kernel_layout(boson)
+    solver = PcgSolver([System(L, Nt, bs)], mode=mode, rtol=1e-15, max_iter=iters, device=DEV)
+    if solver.vec_dtype == torch.complex64:
+        x0 = x0.astype(np.complex64).astype(np.complex128)
+    res = solver.solve(torch.tensor(phi.reshape(bs, -1), dtype=solver.angle_dtype, device=DEV),
+                       torch.tensor(b, dtype=solver.vec_dtype, device=DEV),
+                       x0=torch.tensor(x0, dtype=solver.vec_dtype, device=DEV))
+    assert res.iters.cpu().tolist() == [iters] * bs
+    phi_used = phi.astype(np.float32).astype(np.float64) if solver.angle_dtype == torch.float32 else phi
+    A = lambda v: O.mhm_vec(phi_used, v.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    Pf = lambda v: O.precon_vec(v.reshape(bs, Nt, L * L), O.precon_tau_matrix(Nt)).reshape(bs, -1)
+    d, _, _ = O.pcg_batched_masked(A, b - A(x0), Pf, 1e-15, iters, reference_alias=False)
+    assert relerr(res.x.cpu().numpy().reshape(bs, -1), x0 + d) < tol
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed", "mixed_bf16", "fp32"])
+def test_pcg_initial_guess_solves(mode):
+    """A guess near the solution converges to the same tolerance in fewer
+    iterations; the solution itself needs none; a right-hand side b = 0 gets
+    x = 0 whatever its guess."""
+    from qed_fermion_b200.solver import PcgSolver, System
+    L, Nt, bs = 6, 40, 3
+    boson, b = rand_case(L, Nt, bs, seed=79, kind="piflux")
+    b[2] = 0
+    phi = O.ref_to_kernel_layout(boson)
+    rtol = 1e-5 if mode == "fp32" else 1e-10
+    solver = PcgSolver([System(L, Nt, bs)], mode=mode, rtol=rtol, max_iter=20000, device=DEV)
+    ph = torch.tensor(phi.reshape(bs, -1), dtype=solver.angle_dtype, device=DEV)
+    bt = torch.tensor(b, dtype=solver.vec_dtype, device=DEV)
+    r0 = solver.solve(ph, bt)
+    x = r0.x.clone().view(bs, -1)
+    it0 = r0.iters.cpu().tolist()
+    assert r0.status.cpu().tolist() == [0] * bs and it0[2] == 0
+    rng = np.random.default_rng(6)
+    pert = torch.tensor(1 + 1e-3 * rng.standard_normal(x.shape), device=DEV).to(x.real.dtype)
+    guess = (x * pert).contiguous()
+    guess[2] = 1.0
+    r1 = solver.solve(ph, bt, x0=guess)
+    it1 = r1.iters.cpu().tolist()
+    assert r1.status.cpu().tolist() == [0] * bs
+    assert it1[0] < it0[0] and it1[1] < it0[1] and it1[2] == 0
+    xs = r1.x.view(bs, -1)
+    assert torch.count_nonzero(xs[2]) == 0
+    phi_used = phi.astype(np.float32).astype(np.float64) if solver.angle_dtype == torch.float32 else phi
+    xn = xs.cpu().numpy().astype(np.complex128)
+    r = b - O.mhm_vec(phi_used, xn.reshape(bs, Nt, L * L), L, 0.1).reshape(bs, -1)
+    true_rel = np.linalg.norm(r[:2], axis=1) / np.linalg.norm(b[:2], axis=1)
+    assert np.all(true_rel < (5 * rtol if mode == "fp32" else 2 * rtol)), true_rel
+    r2 = solver.solve(ph, bt, x0=r1.x.clone())
+    assert max(r2.iters.cpu().tolist()) <= {"fp64": 1, "fp32": 3}.get(mode, 0)
+    assert r2.status.cpu().tolist() == [0] * bs
+
+
 def test_pcg_l2_window_changes_no_result():
     """The L2 persisting window is a cache policy only: solves with and without it agree bit
     for bit."""

@@ -29,12 +29,16 @@ def _cuda():
     torch.cuda.set_device(DEV)
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed_bf16"])
-def test_mid_size_trajectory_matches_reference(precision):
+@pytest.mark.parametrize("precision,chrono", [("fp64", None), ("mixed", None), ("mixed_bf16", None),
+                                              ("fp64", "linear"), ("mixed", "last"), ("mixed", "linear")])
+def test_mid_size_trajectory_matches_reference(precision, chrono):
+    """``chrono``: the leapfrog's solves start from the previous solutions
+    instead of zero; the same tolerances hold."""
     from qed_fermion_b200.hmc import HmcSampler
     T = dict(np.load(os.path.join(HERE, "golden", "golden_traj_L12.npz")))
     hmc = HmcSampler(Lx=12, Ltau=120, bs=1, precision=precision, cg_rtol=1e-10, max_iter=50000,
-                     delta_t=float(T["mid_delta_t"]), N_leapfrog=int(T["mid_n_leapfrog"]), device=DEV)
+                     delta_t=float(T["mid_delta_t"]), N_leapfrog=int(T["mid_n_leapfrog"]), device=DEV,
+                     chrono_guess=chrono)
     x, H0, H1, it, err = hmc.leapfrog_proposer5(torch.tensor(T["mid_boson"], device=DEV),
                                                 p0=torch.tensor(T["mid_p0"], device=DEV),
                                                 R=torch.tensor(T["mid_R"], device=DEV))
