@@ -62,6 +62,8 @@ def parse_args(argv=None):
     ap.add_argument("--fp64-steps", type=int, default=5, help="trajectories timed on the plain FP64 path")
     ap.add_argument("--bf16-steps", type=int, default=5,
                     help="trajectories timed with the PCG's vectors stored as bf16 (mixed arithmetic)")
+    ap.add_argument("--f16-steps", type=int, default=5,
+                    help="trajectories timed with the PCG's vectors stored as scaled fp16 (mixed arithmetic)")
     ap.add_argument("--graph-steps", type=int, default=10,
                     help="trajectories timed with each trajectory replayed from a CUDA graph (mixed)")
     ap.add_argument("--chrono-steps", type=int, default=10,
@@ -91,7 +93,7 @@ def parse_args(argv=None):
                     help="time the other benchmark configurations (C2, C4a, C4b, C5), one JSON line each")
     ap.add_argument("--matvec-only", type=int, default=0,
                     help="only time M^dag M on this many right-hand sides (c64; c128 with --mode fp64)")
-    ap.add_argument("--mode", default="mixed", choices=["mixed", "mixed_bf16", "fp32", "fp64"],
+    ap.add_argument("--mode", default="mixed", choices=["mixed", "mixed_bf16", "mixed_f16", "fp32", "fp64"],
                     help="precision of the --solve-only solve or --matvec-only launch")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="the library's static launch shapes instead of the autotuner's timed choice")
@@ -544,6 +546,17 @@ def run_native(args):
         bf16["pcg_bytes_per_site_iteration"] = 2 * 4 + 4 * 8 + 2 * 4
         del hb16
 
+    # --- scaled fp16 vector storage, same workload
+    f16 = None
+    if rank == 0 and args.f16_steps > 0 and not args.quick:
+        hf16 = make("mixed_f16")
+        hf16.boson = hmc.boson.clone()
+        f16 = time_trajectories(hf16, args.f16_steps)
+        f16["path"] = ("mixed precision with the PCG's p and z stored as fp16 pairs scaled by a power of two "
+                       "per vector")
+        f16["pcg_bytes_per_site_iteration"] = 2 * 4 + 4 * 8 + 2 * 4
+        del hf16
+
     # --- Delta H of one shared trajectory: mixed and bf16 storage against FP64
     dH = None
     if rank == 0 and not args.quick:
@@ -558,7 +571,7 @@ def run_native(args):
         del h64
         dHd = (H1d - H0d).cpu()
         dH = {"dH_fp64": dHd.tolist(), "H0": H0d.cpu().tolist()}
-        for name, h in (("mixed", hmc), ("mixed_bf16", make("mixed_bf16")),
+        for name, h in (("mixed", hmc), ("mixed_bf16", make("mixed_bf16")), ("mixed_f16", make("mixed_f16")),
                         ("mixed_chrono_linear", make("mixed", chrono_guess="linear"))):
             _, H0m, H1m, _, _ = h.leapfrog_proposer5(x0.to(torch.float32), p0=p0.to(torch.float32), R=R)
             dHm = (H1m - H0m).cpu()
@@ -663,7 +676,7 @@ def run_native(args):
                                        if fp64 and "dropin" in fp64 else None),
             "pcg_launch_shape": ({k: hmc.solver.tuned[k] for k in ("by", "slab", "stage", "chunk")}
                                  if hmc.solver.tuned else None),
-            "bf16": bf16, "graph": graph, "chrono": chrono, "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate,
+            "bf16": bf16, "f16": f16, "graph": graph, "chrono": chrono, "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate,
             "acceptance_vs_fp64": acc, **result,
         }
         print(json.dumps(line), flush=True)
@@ -702,7 +715,7 @@ def run_solve_only(args):
     it = int(res.iters.max())
     n = L * L * Lt * bs
     # bytes per site and iteration: 7 vector accesses and the two angles
-    bps = {"mixed": 64, "fp32": 64, "fp64": 128, "mixed_bf16": 48}[args.mode]
+    bps = {"mixed": 64, "fp32": 64, "fp64": 128, "mixed_bf16": 48, "mixed_f16": 48}[args.mode]
     print(json.dumps({"solve_only": True, "mode": args.mode, "lattice": [L, L, Lt], "rhs": bs, "iters": it,
                       "ms": ms, "us_per_iter": ms * 1e3 / max(it, 1), "bytes_per_site_iter": bps,
                       "algorithmic_GBps": n * bps * it / (ms / 1e3) / 1e9}), flush=True)

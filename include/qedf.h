@@ -262,6 +262,9 @@ typedef struct {
                                  preconditioned residual z stored as bf16 pairs (4 bytes
                                  per complex number); r, M^dag M p and the float part of x
                                  stay float, as does the arithmetic */
+#define QEDF_PCG_MIXED_F16 4  /* as QEDF_PCG_MIXED_BF16 with fp16 pairs, each vector scaled
+                                 by a power of two taken from the residual's norm, so that
+                                 its entries keep fp16's 11-bit significand */
 
 typedef struct {
   int mode;           /* QEDF_PCG_* */
@@ -289,14 +292,14 @@ typedef struct {
                          0 (default) or -1: the engine that loads them directly */
   int x_init;         /* 1: x holds an initial guess on entry; the solve starts from the
                          residual b - A x, computed in the high precision (double for
-                         MIXED / MIXED_BF16 / PLAIN_F64).  A right-hand side with b = 0
+                         MIXED / MIXED_BF16 / MIXED_F16 / PLAIN_F64).  A right-hand side with b = 0
                          gets x = 0.  0 (default): x starts at 0, as in the reference */
 } qedf_pcg_opts;
 
 /* Bytes of device workspace qedf_pcg_solve needs for these systems. */
 int64_t qedf_pcg_workspace_bytes(const qedf_system* sys, int nsys, const qedf_pcg_opts* opts);
 
-/* Solve.  boson: packed angles (float for PLAIN_F32 / MIXED / MIXED_BF16,
+/* Solve.  boson: packed angles (float for PLAIN_F32 / MIXED / MIXED_BF16 / MIXED_F16,
  * double for PLAIN_F64); b, x: packed vectors (complex64 for PLAIN_F32,
  * complex128 otherwise); iters, relres, status: device arrays with one entry per
  * right-hand side (total over systems).  relres is the last measured relative

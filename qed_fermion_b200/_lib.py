@@ -26,6 +26,7 @@ QEDF_PCG_PLAIN_F32 = 0
 QEDF_PCG_PLAIN_F64 = 1
 QEDF_PCG_MIXED = 2
 QEDF_PCG_MIXED_BF16 = 3
+QEDF_PCG_MIXED_F16 = 4
 
 
 class QedfSystem(ctypes.Structure):

@@ -166,7 +166,7 @@ def pcg_choice(systems, mode, use_precon=True, dtau=0.1, iters=100, force=False,
         if hit is not None:
             return hit
     device = torch.device("cuda", torch.cuda.current_device())
-    stages = [True, False] if mode in ("mixed", "fp32", "mixed_bf16") else [False]
+    stages = [True, False] if mode in ("mixed", "fp32", "mixed_bf16", "mixed_f16") else [False]
     chunks = [16, 32] if mode != "fp64" and max(s.Ltau for s in systems) <= 500 else [16]
     cands = [(by, T, st, ch) for by in tile_heights([s.Lx for s in systems]) for T in slab_candidates(systems)
              for st in stages for ch in chunks]

@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -153,6 +154,52 @@ __device__ __forceinline__ Cx<R> round_st(Cx<R> v) {
   } else {
     return v;
   }
+}
+
+// Scaled fp16 storage (the PCG's F16 option): a vector is kept as fp16 pairs
+// of v / sc, with sc a power of two chosen per vector from its norm, so the
+// stored values sit in fp16's range whatever the residual's size and keep its
+// 11-bit significand.  Scaling by a power of two is exact, so sc * (stored)
+// is exactly the value the registers hold after round_st.  The overloads for
+// the other storage types ignore the scale.
+__device__ __forceinline__ void ld2s(const __half* p, Cx<float>& a, Cx<float>& b, float sc) {
+  const uint2 q = *reinterpret_cast<const uint2*>(p);
+  const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&q.x));
+  const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
+  a = mk<float>(lo.x * sc, lo.y * sc);
+  b = mk<float>(hi.x * sc, hi.y * sc);
+}
+__device__ __forceinline__ void st2s(__half* p, Cx<float> a, Cx<float> b, float inv) {
+  const __half2 lo = __floats2half2_rn(a.re * inv, a.im * inv);
+  const __half2 hi = __floats2half2_rn(b.re * inv, b.im * inv);
+  uint2 q;
+  q.x = *reinterpret_cast<const unsigned*>(&lo);
+  q.y = *reinterpret_cast<const unsigned*>(&hi);
+  *reinterpret_cast<uint2*>(p) = q;
+}
+template <typename S, typename R>
+__device__ __forceinline__ void ld2s(const S* p, Cx<R>& a, Cx<R>& b, R) { ld2s(p, a, b); }
+template <typename S, typename R>
+__device__ __forceinline__ void st2s(S* p, Cx<R> a, Cx<R> b, R) { st2s(p, a, b); }
+template <typename S, typename R>
+__device__ __forceinline__ Cx<R> round_st(Cx<R> v, R sc, R inv) {
+  if constexpr (std::is_same<S, __half>::value) {
+    const float2 f = __half22float2(__floats2half2_rn(v.re * inv, v.im * inv));
+    return mk<R>(f.x * sc, f.y * sc);
+  } else {
+    return round_st<S>(v);
+  }
+}
+// the power-of-two scale of a vector with squared norm nn: about its norm
+// / 1024, so entries of vectors of 10^3-10^7 sites stay well inside fp16's
+// normal range; 1 for a zero or non-finite norm
+__device__ __forceinline__ float st_scale(double nn) {
+  if (!(nn > 0.0) || !isfinite(nn)) return 1.0f;
+  int e;
+  frexp(nn, &e);                         // nn in [2^(e-1), 2^e)
+  int es = ((e - 1) >> 1) - 10;          // floor(log2 |v|) - 10
+  es = es < -120 ? -120 : (es > 120 ? 120 : es);
+  return ldexpf(1.0f, es);
 }
 
 // four reals (angles or forces of two sites, both components)

@@ -108,7 +108,7 @@ struct PcgSys {
 struct PcgParams {
   int nsys, nrhs, unitsA, unitsE, CH;
   PcgSys sys[PCG_MAX_SYS];
-  int mode;  // QEDF_PCG_PLAIN_F32, QEDF_PCG_PLAIN_F64, QEDF_PCG_MIXED, QEDF_PCG_MIXED_BF16
+  int mode;  // QEDF_PCG_PLAIN_F32, QEDF_PCG_PLAIN_F64, QEDF_PCG_MIXED, QEDF_PCG_MIXED_BF16, QEDF_PCG_MIXED_F16
   int xs;    // allow the warp-shuffle engine for the single-precision iterations
   int stage; // 1: allow the staged operator engine (EC_STAGE) where its shared memory fits
   int stage_off;  // bytes: start of the operator passes' slice stages in dynamic shared memory

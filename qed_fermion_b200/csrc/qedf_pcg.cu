@@ -186,6 +186,15 @@ struct RhsState {
   double red[96];
 };
 
+// Per-block copy of the storage scales of z and of the two p buffers (scaled
+// fp16 storage only), identical in all blocks: each is set from the squared
+// residual norm, which every block holds, before the pass that writes the
+// vector, and is read by the passes that load it.
+struct StScales {
+  float z[PCG_MAX_RHS], p[2][PCG_MAX_RHS];
+};
+struct StNoScales {};
+
 // Optional phase timing (block 0, thread 0): prof[k] accumulates clock64 cycles of
 //   0 init, 1 operator phase work, 2 wait after it, 3 elementwise phase work,
 //   4 wait after it, 5 reliable updates (work + waits), 6 iterations, 7 total
@@ -219,15 +228,28 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   constexpr bool STG_S = (ECS & EC_STAGE) != 0;
   static_assert(!STG_S || (STASH_S && !XS_S), "the staged engine keeps y_t in the stash");
   // storage of the search direction p and the preconditioned residual z: the
-  // iteration precision, or bf16 pairs (EC_BF16, mixed mode).
-  // r, M^dag M p and x_lo always keep the iteration precision, so that the
-  // residual recurrence r -= alpha M^dag M p stays that of x += alpha p.
+  // iteration precision, bf16 pairs (EC_BF16) or scaled fp16 pairs (EC_F16),
+  // both mixed-mode options.  r, M^dag M p and x_lo always keep the iteration
+  // precision, so that the residual recurrence r -= alpha M^dag M p stays that
+  // of x += alpha p.
   constexpr bool BF = (ECS & EC_BF16) != 0;
-  using SP = typename std::conditional<BF, bf16, RS>::type;
-  static_assert(!BF || (sizeof(RS) == 4 && !std::is_same<RS, RH>::value && !XS_S),
-                "bf16 storage is a mixed-precision mode");
+  constexpr bool H16 = (ECS & EC_F16) != 0;
+  constexpr bool LOWP = BF || H16;
+  using SP = typename std::conditional<BF, bf16, typename std::conditional<H16, __half, RS>::type>::type;
+  static_assert(!LOWP || (sizeof(RS) == 4 && !std::is_same<RS, RH>::value && !XS_S && !(BF && H16)),
+                "bf16 and fp16 storage are mixed-precision modes");
   extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ RhsState st;
+  __shared__ typename std::conditional<H16, StScales, StNoScales>::type scl;
+  // scales of z and of p buffer `par` (1 for every other storage type)
+  auto sc_z = [&](int v) -> RS {
+    if constexpr (H16) return (RS)scl.z[v];
+    else return (RS)1;
+  };
+  auto sc_p = [&](int par, int v) -> RS {
+    if constexpr (H16) return (RS)scl.p[par][v];
+    else return (RS)1;
+  };
   __shared__ unsigned long long stg_bar[2];
   constexpr bool MIXED = !std::is_same<RS, RH>::value;
   // lattice side: compiled in (every system has it) or per system
@@ -288,7 +310,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
   // ---- BC-type elementwise pass over one unit --------------------------------
   // kind 0: init (x = 0 unless it holds an initial guess, r = b, bb); 1:
   // iteration update; 2: preconditioner only (after a reliable update or the
-  // initial guess's residual).  A unit is CHC sites of one right-hand side over
+  // initial guess's residual); 3: preconditioner only, r^dag z into the rz
+  // slot (scaled fp16 init).  A unit is CHC sites of one right-hand side over
   // all tau; a thread handles two neighbouring sites (one 16-byte access per
   // vector in single precision) in every (blockDim/PPR)-th row.  r of the unit
   // stays in shared memory for the tau-stencil of the preconditioner, whose
@@ -382,9 +405,13 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
 #pragma unroll
     for (int d = 0; d < 7; ++d) cmid[d] = (RS)c_pre.middle[d];
     RS bpart = 0;  // this thread's r^dag z in the iteration precision
+    // scaled fp16: the scale of z follows from |r|, known only after the init
+    // pass, so that pass leaves z to a kind-3 pass
+    const bool zpass = !(H16 && kind == 0);
+    const RS szv = sc_z(v), izv = (RS)1 / szv;  // powers of two: exact
 #pragma unroll 2
     for (int t = tid / PPR; t < Nt; t += rstep) {
-      if (!jon) continue;
+      if (!jon || !zpass) continue;
       Cx<RS> r0, r1;
       ld2c(reinterpret_cast<const RS*>(rsm + t * CHC + 2 * j), r0, r1);
       Cx<RS> z0 = r0, z1 = r1;
@@ -414,15 +441,16 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
           }
         }
         const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
-        z0 = round_st<SP>(z0);
-        z1 = round_st<SP>(z1);
-        st2s(z + i2, z0, z1);
-      } else if (BF) {
-        // the bf16 engine reads z even without a preconditioner: z = r, rounded
+        z0 = round_st<SP>(z0, szv, izv);
+        z1 = round_st<SP>(z1, szv, izv);
+        st2s(z + i2, z0, z1, izv);
+      } else if (LOWP) {
+        // the narrow-storage engines read z even without a preconditioner:
+        // z = r, rounded
         const int64_t i2 = 2 * (base + (int64_t)t * Vs + c0 + 2 * j);
-        z0 = round_st<SP>(z0);
-        z1 = round_st<SP>(z1);
-        st2s(z + i2, z0, z1);
+        z0 = round_st<SP>(z0, szv, izv);
+        z1 = round_st<SP>(z1, szv, izv);
+        st2s(z + i2, z0, z1, izv);
       }
       bpart = fma(r0.re, z0.re, fma(r0.im, z0.im, fma(r1.re, z1.re, fma(r1.im, z1.im, bpart))));
     }
@@ -436,6 +464,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         atomicAdd(acc.rz + slot * NV + v, sb);
       } else if (kind == 1) {
         atomicAdd(acc.rr + slot * NV + v, sc);
+        atomicAdd(acc.rz + slot * NV + v, sb);
+      } else if (kind == 3) {
         atomicAdd(acc.rz + slot * NV + v, sb);
       } else {
         atomicAdd(acc.ru_rz + v, sb);
@@ -470,8 +500,12 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     RS* xl = xs + vb;
     const SP* pold = reinterpret_cast<const SP*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
     SP* pnew = reinterpret_cast<SP*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
+    // storage scales (1 unless scaled fp16): z, p_old, and p_new's, set to
+    // z's at the start of the phase
+    const RS s_z = sc_z(v), s_po = sc_p((st.iters[v] & 1) ^ 1, v);
+    const RS s_pn = sc_p(st.iters[v] & 1, v), i_pn = (RS)1 / s_pn;
     const SP* zz = (guess_pass ? reinterpret_cast<const SP*>(xs)
-                               : (S.precon || BF) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
+                               : (S.precon || LOWP) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
     RS* O = Op + vb;
     const RS t1 = (RS)p.t1, th = (RS)p.th, Cb = (RS)p.Cb;
     Cx<RS> X0[BY][2], X1[BY][2], Y[BY][2];
@@ -479,10 +513,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     double pap = 0;
     auto getp = [&](Cx<RS> (&X)[BY][2], int t, bool own) {
       if (!E.on) return;
-      E.load_st(X, zz + t * sv);
+      E.load_st(X, zz + t * sv, s_z);
       if (has_old) {
         Cx<RS> T0[BY][2];
-        E.load_st(T0, pold + t * sv);
+        E.load_st(T0, pold + t * sv, s_po);
         if (own && pend) {
           Cx<RS> XL[BY][2];
           E.load_coherent(XL, xl + t * sv);
@@ -501,14 +535,14 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
           for (int c = 0; c < 2; ++c) {
             X[q][c].re = fma(beta, T0[q][c].re, X[q][c].re);
             X[q][c].im = fma(beta, T0[q][c].im, X[q][c].im);
-            X[q][c] = round_st<SP>(X[q][c]);
+            X[q][c] = round_st<SP>(X[q][c], s_pn, i_pn);
           }
       }
     };
     const int tp = (a - 1 + Nt) % Nt;
     getp(X0, tp, false);
     getp(X1, a, true);
-    if (E.on) E.store_st(pnew + a * sv, X1);
+    if (E.on) E.store_st(pnew + a * sv, X1, i_pn);
     A ang[BY][4];
     if constexpr (!PHS_S) E.load_angles(ang, phi + a * sv);
     E.phases(phi + tp * sv, t1, th);
@@ -519,7 +553,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     for (int t = a; t < bnd; ++t) {
       const int tn = (t + 1) % Nt;
       getp(X1, tn, t + 1 < bnd);
-      if (E.on && t + 1 < bnd) E.store_st(pnew + tn * sv, X1);
+      if (E.on && t + 1 < bnd) E.store_st(pnew + tn * sv, X1, i_pn);
       if constexpr (!PHS_S) {
         E.phases_from(ang, t1, th);
         if (t + 1 < bnd) E.load_angles(ang, phi + (t + 1) * sv);
@@ -582,8 +616,12 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     RS* xl = xs + vb;
     const SP* pold = reinterpret_cast<const SP*>((st.iters[v] & 1) ? p.p0 : p.p1) + vb;
     SP* pnew = reinterpret_cast<SP*>((st.iters[v] & 1) ? p.p1 : p.p0) + vb;
+    // storage scales (1 unless scaled fp16): z, p_old, and p_new's, set to
+    // z's at the start of the phase
+    const RS s_z = sc_z(v), s_po = sc_p((st.iters[v] & 1) ^ 1, v);
+    const RS s_pn = sc_p(st.iters[v] & 1, v), i_pn = (RS)1 / s_pn;
     const SP* zz = (guess_pass ? reinterpret_cast<const SP*>(xs)
-                               : (S.precon || BF) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
+                               : (S.precon || LOWP) ? zbuf : reinterpret_cast<const SP*>(r)) + vb;
     RS* O = Op + vb;
     const RS t1 = (RS)p.t1, th = (RS)p.th, Cb = (RS)p.Cb;
     // slots of the iteration precision; z and p_old may be narrower
@@ -607,10 +645,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     // also x_lo += alpha_old p_old
     auto getp = [&](Cx<RS> (&X)[BY][2], int j, bool own) {
       if (!E.on) return;
-      E.load_st(X, reinterpret_cast<const SP*>(stg.slot(j, 0)));
+      E.load_st(X, reinterpret_cast<const SP*>(stg.slot(j, 0)), s_z);
       if (has_old) {
         Cx<RS> T0[BY][2];
-        E.load_st(T0, reinterpret_cast<const SP*>(stg.slot(j, 1)));
+        E.load_st(T0, reinterpret_cast<const SP*>(stg.slot(j, 1)), s_po);
         if (own && pend) {
           Cx<RS> XL[BY][2];
           E.load_coherent(XL, reinterpret_cast<const RS*>(stg.slot(j, 2)));
@@ -629,7 +667,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
           for (int c = 0; c < 2; ++c) {
             X[q][c].re = fma(beta, T0[q][c].re, X[q][c].re);
             X[q][c].im = fma(beta, T0[q][c].im, X[q][c].im);
-            X[q][c] = round_st<SP>(X[q][c]);
+            X[q][c] = round_st<SP>(X[q][c], s_pn, i_pn);
           }
       }
     };
@@ -641,7 +679,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     getp(X0, 0, false);
     wait(1);
     getp(X1, 1, true);
-    if (E.on) E.store_st(pnew + a * sv, X1);
+    if (E.on) E.store_st(pnew + a * sv, X1, i_pn);
     A ang[BY][4];
     if constexpr (!PHS_S) E.load_angles(ang, phi + a * sv);
     E.phases(phi + tp * sv, t1, th);  // block barrier: stage 0 is read
@@ -655,7 +693,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       issue(i + 3);  // into the buffer of stage i + 1, read before the last barriers
       wait(i + 2);
       getp(X1, i + 2, t + 1 < bnd);
-      if (E.on && t + 1 < bnd) E.store_st(pnew + tn * sv, X1);
+      if (E.on && t + 1 < bnd) E.store_st(pnew + tn * sv, X1, i_pn);
       if constexpr (!PHS_S) {
         E.phases_from(ang, t1, th);
         if (t + 1 < bnd) E.load_angles(ang, phi + (t + 1) * sv);
@@ -761,7 +799,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     const SP* pl = reinterpret_cast<const SP*>((st.iters[v] & 1) ? p.p0 : p.p1);  // p of the last iteration
     const RS al = (RS)st.alpha[v];
     Cx<RS> p0v, p1v;
-    ld2s(pl + i2, p0v, p1v);
+    ld2s(pl + i2, p0v, p1v, sc_p((st.iters[v] & 1) ^ 1, v));
     l0 = mk<RS>(fma(al, p0v.re, l0.re), fma(al, p0v.im, l0.im));
     l1 = mk<RS>(fma(al, p1v.re, l1.re), fma(al, p1v.im, l1.im));
   };
@@ -854,6 +892,20 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     }
     __syncthreads();
   }
+  if constexpr (H16) {
+    // z = P r now that |r| = |b| fixes z's scale; r^dag z into the rz slot,
+    // which the init pass left at zero
+    if (ok) {
+      for (int v = tid; v < NV; v += blockDim.x) scl.z[v] = st_scale(st.rr[v]);
+      __syncthreads();
+      for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) elementwise(3, u, 0);
+      ok = grid_barrier(p.bar, nblk, budget, bar_target);
+    }
+    if (ok) {
+      for (int v = tid; v < NV; v += blockDim.x) st.rz[v] = acc.rz[v];
+      __syncthreads();
+    }
+  }
   // initial guess: a right-hand side with b = 0 gets x = 0.  Mixed modes start
   // the others with a reliable update (r = b - A x in double, z = P r); plain
   // modes with one pass of the iteration's own two phases on p = x (guess
@@ -911,6 +963,11 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
         if (st.ru[v]) operator_unit_true_residual(u);
       }
       if (!(ok = grid_barrier(p.bar, nblk, budget, bar_target))) break;
+      if constexpr (H16) {
+        for (int v = tid; v < NV; v += blockDim.x)
+          if (st.ru[v]) scl.z[v] = st_scale(acc.ru_rr[v]);
+        __syncthreads();
+      }
       for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) {
         int s, v, c0, c1;
         unitE(u, s, v, c0, c1);
@@ -942,7 +999,11 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     if (!st.any_active || it >= p.max_iter) break;
 
     // ---- phase A
-    for (int v = tid; v < NV; v += blockDim.x) st.beta[v] = st.iters[v] > 0 ? st.rz[v] / st.rzold[v] : 0.0;
+    for (int v = tid; v < NV; v += blockDim.x) {
+      st.beta[v] = st.iters[v] > 0 ? st.rz[v] / st.rzold[v] : 0.0;
+      if constexpr (H16)
+        if (st.active[v]) scl.p[st.iters[v] & 1][v] = scl.z[v];  // the buffer p_new goes to
+    }
     __syncthreads();
     // (the guess pass uses the pAp slot of odd iterations, so that its BC
     // phase clears the slot of iteration 0)
@@ -969,7 +1030,10 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     // alpha of inactive systems stays that of their last iteration: a pending
     // x update still uses it
     for (int v = tid; v < NV; v += blockDim.x)
-      if (st.active[v]) st.alpha[v] = guess_pass ? 1.0 : st.rz[v] / acc.pAp[aslot * NV + v];
+      if (st.active[v]) {
+        st.alpha[v] = guess_pass ? 1.0 : st.rz[v] / acc.pAp[aslot * NV + v];
+        if constexpr (H16) scl.z[v] = st_scale(st.rr[v]);  // |r| before this update
+      }
     __syncthreads();
     for (int u = blockIdx.x; u < p.unitsE; u += gridDim.x) {
       int s, v, c0, c1;
@@ -1029,7 +1093,7 @@ static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 template <typename RS>
 static size_t pcg_stage_bytes(int L) { return 2 * 3 * (size_t)L * L * 2 * sizeof(RS); }
 
-// (MIXED_BF16 keeps r, M^dag M p and x_lo in float; its p and z buffers use
+// (MIXED_BF16 and MIXED_F16 keep r, M^dag M p and x_lo in float; their p and z buffers use
 // half of their float-sized room)
 int pcg_storage_bytes(int mode) { return mode == QEDF_PCG_PLAIN_F64 ? 8 : 4; }
 
@@ -1058,7 +1122,7 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
   std::memset(&p, 0, sizeof(p));
   if (!sys || !o || nsys <= 0 || nsys > PCG_MAX_SYS) return QEDF_ERR_ARG;
   if (o->mode != QEDF_PCG_PLAIN_F32 && o->mode != QEDF_PCG_PLAIN_F64 && o->mode != QEDF_PCG_MIXED &&
-      o->mode != QEDF_PCG_MIXED_BF16)
+      o->mode != QEDF_PCG_MIXED_BF16 && o->mode != QEDF_PCG_MIXED_F16)
     return QEDF_ERR_ARG;
   p.mode = o->mode;
   p.nsys = nsys;
@@ -1158,7 +1222,7 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
 // barrier words, contiguous from p.acc).
 size_t pcg_carve(PcgParams& p, int sloppy_bytes, void* workspace, size_t* zero_bytes) {
   const size_t vecb = align_up((size_t)p.nvec_total * 2 * sloppy_bytes, 256);
-  const bool mixed = p.mode == QEDF_PCG_MIXED || p.mode == QEDF_PCG_MIXED_BF16;
+  const bool mixed = p.mode == QEDF_PCG_MIXED || p.mode == QEDF_PCG_MIXED_BF16 || p.mode == QEDF_PCG_MIXED_F16;
   const int nv = mixed ? 6 : 5;
   const size_t accb = align_up(sizeof(double) * ACC_PER_RHS * p.nrhs, 256);
   const size_t barb = 256;
@@ -1400,6 +1464,14 @@ static int launch_pcg_by(PcgParams& p, cudaStream_t st) {
       if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
         return launch_pcg_fl<float, double, float, BY, EC_BF16, 0>(p, st);
       return launch_pcg_t<float, double, float, BY, EC_BF16, EC_NOSTASH>(p, st);
+    case QEDF_PCG_MIXED_F16:
+      if (p.stage && fits_staged<float, 0>(Lmax, BY) && fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
+        return launch_pcg_fl<float, double, float, BY, EC_STAGE | EC_F16, EC_PHS>(p, st);
+      if (fits(slice_smem_bytes<double, EC_PHS>(Lmax, BY, 2)))
+        return launch_pcg_fl<float, double, float, BY, EC_F16, EC_PHS>(p, st);
+      if (fits(slice_smem_bytes<double, 0>(Lmax, BY, 2)))
+        return launch_pcg_fl<float, double, float, BY, EC_F16, 0>(p, st);
+      return launch_pcg_t<float, double, float, BY, EC_F16, EC_NOSTASH>(p, st);
   }
   return QEDF_ERR_ARG;
 }

@@ -56,9 +56,12 @@ struct MaxThreads {
 //   EC_BF16    (PCG, mixed mode) the search direction p and the preconditioned
 //              residual z are stored as bf16 pairs; the arithmetic stays in
 //              single precision
+//   EC_F16     (PCG, mixed mode) p and z stored as fp16 pairs scaled by a power
+//              of two per vector (st_scale); the arithmetic stays in single
+//              precision
 //   EC_L(l)    (bits 8 and up) the lattice side fixed at compile time, so the
 //              engine's index arithmetic folds into constants; 0 = run-time L
-enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_STAGE = 8, EC_BF16 = 16 };
+enum { EC_PHS = 1, EC_NOSTASH = 2, EC_XS = 4, EC_STAGE = 8, EC_BF16 = 16, EC_F16 = 32 };
 __host__ __device__ constexpr int EC_L(int l) { return l << 8; }
 __host__ __device__ constexpr int ec_fixed_l(int ec) { return ec >> 8; }
 // Lattice sides with engines compiled for their size: the benchmark
@@ -218,6 +221,17 @@ struct Slice {
   __device__ __forceinline__ void store_st(S* slice, const Cx<R> (&v)[BY][2]) const {
 #pragma unroll
     for (int r = 0; r < BY; ++r) st2s(slice + 2 * ((y0 + r) * L + x0), v[r][0], v[r][1]);
+  }
+  // scaled storage (fp16: stored value times sc; other types ignore the scale)
+  template <typename S>
+  __device__ __forceinline__ void load_st(Cx<R> (&v)[BY][2], const S* slice, R sc) const {
+#pragma unroll
+    for (int r = 0; r < BY; ++r) ld2s(slice + 2 * ((y0 + r) * L + x0), v[r][0], v[r][1], sc);
+  }
+  template <typename S>
+  __device__ __forceinline__ void store_st(S* slice, const Cx<R> (&v)[BY][2], R inv) const {
+#pragma unroll
+    for (int r = 0; r < BY; ++r) st2s(slice + 2 * ((y0 + r) * L + x0), v[r][0], v[r][1], inv);
   }
 
   // thread-private parking of one block (no synchronisation needed)

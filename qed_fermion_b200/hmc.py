@@ -15,7 +15,8 @@ Precision ("precision" argument):
   "mixed" float32 angles and momenta (as the reference stores them), PCG in
           float with double reliable updates, float force, and the
           Hamiltonian, Delta H and the Metropolis test in double;
-  "mixed_bf16" as "mixed", with the PCG's iteration vectors stored as bf16;
+  "mixed_bf16" as "mixed", with the PCG's p and z stored as bf16;
+  "mixed_f16" as "mixed", with the PCG's p and z stored as scaled fp16;
   "fp32"  everything in single precision (the reference's own GPU choice).
 
 ``chrono_guess`` ("last" or "linear") starts each leapfrog solve after the
@@ -43,7 +44,7 @@ from . import _lib, ops
 from .fourier_mass import FourierMass
 from .solver import PcgSolver, System
 
-PRECISIONS = ("fp64", "mixed", "mixed_bf16", "fp32")
+PRECISIONS = ("fp64", "mixed", "mixed_bf16", "mixed_f16", "fp32")
 
 
 def ref_to_kernel(boson: torch.Tensor) -> torch.Tensor:
@@ -97,12 +98,13 @@ class HmcSampler:
         self.use_precon = use_precon and Ltau >= 26
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         self.dtype = torch.float64 if precision == "fp64" else torch.float32
-        self.cdtype = torch.complex128 if precision in ("fp64", "mixed", "mixed_bf16") else torch.complex64
+        self.cdtype = torch.complex128 if precision in ("fp64", "mixed", "mixed_bf16", "mixed_f16") else torch.complex64
         self.delta_t_tensor = torch.full((bs,), float(delta_t), device=self.device, dtype=torch.float64)
         self.generator = torch.Generator(device=self.device)
         if seed is not None:
             self.generator.manual_seed(seed)
-        solver_mode = {"fp64": "fp64", "mixed": "mixed", "mixed_bf16": "mixed_bf16", "fp32": "fp32"}[precision]
+        solver_mode = {"fp64": "fp64", "mixed": "mixed", "mixed_bf16": "mixed_bf16", "mixed_f16": "mixed_f16",
+                       "fp32": "fp32"}[precision]
         self.solver = PcgSolver([System(Lx, Ltau, bs, False)], mode=solver_mode, rtol=cg_rtol, max_iter=max_iter,
                                 dtau=dtau, use_precon=self.use_precon, ru_interval=ru_interval,
                                 ru_delta=ru_delta, device=self.device, tune=autotune)

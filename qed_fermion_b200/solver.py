@@ -16,7 +16,10 @@ Precision modes:
           residual z stored as bf16 pairs, 4 bytes per complex number; r,
           M^dag M p and the float part of x stay float, so the residual
           recurrence matches the x updates; convergence is still decided on
-          the double-precision true residual.
+          the double-precision true residual;
+  "mixed_f16" as "mixed_bf16" with fp16 pairs, each vector scaled by a power
+          of two taken from the residual's norm (fp16's 11-bit significand
+          instead of bf16's 8 bits, at the same 4 bytes).
 """
 from __future__ import annotations
 
@@ -29,10 +32,11 @@ from . import _lib
 from .ops import ptr, stream_handle
 
 MODES = {"fp32": _lib.QEDF_PCG_PLAIN_F32, "fp64": _lib.QEDF_PCG_PLAIN_F64, "mixed": _lib.QEDF_PCG_MIXED,
-         "mixed_bf16": _lib.QEDF_PCG_MIXED_BF16}
+         "mixed_bf16": _lib.QEDF_PCG_MIXED_BF16, "mixed_f16": _lib.QEDF_PCG_MIXED_F16}
 VEC_DTYPE = {"fp32": torch.complex64, "fp64": torch.complex128, "mixed": torch.complex128,
-             "mixed_bf16": torch.complex128}
-ANGLE_DTYPE = {"fp32": torch.float32, "fp64": torch.float64, "mixed": torch.float32, "mixed_bf16": torch.float32}
+             "mixed_bf16": torch.complex128, "mixed_f16": torch.complex128}
+ANGLE_DTYPE = {"fp32": torch.float32, "fp64": torch.float64, "mixed": torch.float32, "mixed_bf16": torch.float32,
+               "mixed_f16": torch.float32}
 
 
 @dataclass(frozen=True)

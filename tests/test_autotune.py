@@ -43,7 +43,7 @@ def _solve_case(L, Nt, nrhs, seed):
 
 @pytest.mark.gpu
 @pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA device")
-@pytest.mark.parametrize("mode", ["mixed", "fp64", "mixed_bf16"])
+@pytest.mark.parametrize("mode", ["mixed", "fp64", "mixed_bf16", "mixed_f16"])
 def test_every_pcg_candidate_meets_rtol(mode, tmp_path, monkeypatch):
     from qed_fermion_b200 import build
     from qed_fermion_b200.solver import PcgSolver

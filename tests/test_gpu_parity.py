@@ -369,7 +369,7 @@ def test_pcg_initial_guess_iterates_match_oracle(mode, tol, iters):
     assert relerr(res.x.cpu().numpy().reshape(bs, -1), x0 + d) < tol
 
 
-@pytest.mark.parametrize("mode", ["fp64", "mixed", "mixed_bf16", "fp32"])
+@pytest.mark.parametrize("mode", ["fp64", "mixed", "mixed_bf16", "mixed_f16", "fp32"])
 def test_pcg_initial_guess_solves(mode):
     """A guess near the solution converges to the same tolerance in fewer
     iterations; the solution itself needs none; a right-hand side b = 0 gets

@@ -63,15 +63,18 @@ def test_pcg_staged_engine_is_bit_identical(mode, systems):
     assert torch.allclose(out[0][2], out[1][2], rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("mode", ["mixed_bf16", "mixed_f16"])
+@pytest.mark.parametrize("stage", [False, True])
 @pytest.mark.parametrize("L,Nt,nrhs,kind", [(12, 40, 2, "piflux"), (48, 48, 2, "piflux"), (20, 14, 1, "piflux")])
-def test_pcg_bf16_storage_meets_rtol_on_true_residual(L, Nt, nrhs, kind):
-    """Vectors stored as bf16 pairs, float arithmetic, double reliable updates:
-    the returned x meets rtol = 1e-10 on the true residual (the oracle's
-    operator on the same angles) and agrees with the oracle's solution."""
+def test_pcg_bf16_storage_meets_rtol_on_true_residual(L, Nt, nrhs, kind, stage, mode):
+    """p and z stored as bf16 pairs or scaled fp16 pairs, float arithmetic,
+    double reliable updates, on either operator engine: the returned x meets
+    rtol = 1e-10 on the true residual (the oracle's operator on the same
+    angles) and agrees with the plain mixed solution."""
     from qed_fermion_b200.solver import PcgSolver, System
     phi, b = _case(L, Nt, nrhs, seed=L * Nt)
-    s = PcgSolver([System(L, Nt, nrhs)], mode="mixed_bf16", rtol=1e-10, max_iter=20000, device=DEV,
-                  timeout_ms=500.0)
+    s = PcgSolver([System(L, Nt, nrhs)], mode=mode, rtol=1e-10, max_iter=20000, device=DEV,
+                  timeout_ms=500.0, stage=stage)
     res = s.solve(torch.tensor(phi, dtype=torch.float32, device=DEV), torch.tensor(b, device=DEV))
     assert res.status.cpu().tolist() == [0] * nrhs
     x = res.x.cpu().numpy().reshape(nrhs, -1)

@@ -29,7 +29,7 @@ def _cuda():
     torch.cuda.set_device(DEV)
 
 
-@pytest.mark.parametrize("precision,chrono", [("fp64", None), ("mixed", None), ("mixed_bf16", None),
+@pytest.mark.parametrize("precision,chrono", [("fp64", None), ("mixed", None), ("mixed_bf16", None), ("mixed_f16", None),
                                               ("fp64", "linear"), ("mixed", "last"), ("mixed", "linear")])
 def test_mid_size_trajectory_matches_reference(precision, chrono):
     """``chrono``: the leapfrog's solves start from the previous solutions
