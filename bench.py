@@ -656,6 +656,9 @@ def run_native(args):
                "s_per_unit": u}
 
     if rank == 0:
+        for leg in (f16, bf16, graph, chrono):
+            if leg and fp64:
+                leg["speedup_vs_fp64"] = leg["value"] / fp64["value"]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed * 1e3 / args.steps, "higher_is_better": True,
