@@ -883,7 +883,7 @@ def run_configs(args):
         ms, _ = timed(lambda: ops.apply_operator("mhm", phi_p, b_p, L, 0.1, out=out), reps=20)
         emit({"config": "C2", "what": f"M^dag M {prec}, 1 rhs (a single launch of 138,240 sites)", "ms": ms,
               "GBps": bps * N / (ms / 1e3) / 1e9})
-    for mode in ("mixed", "fp64"):
+    for mode in ("mixed", "mixed_f16", "fp64"):
         s = PcgSolver([System(L, Lt, 1)], mode=mode, rtol=1e-8, max_iter=100000, device=dev, tune=True)
         args_ = (phi.reshape(-1).to(s.angle_dtype), b.reshape(-1).to(s.vec_dtype))
         ms, res = timed(lambda: s.solve(*args_))
@@ -898,6 +898,11 @@ def run_configs(args):
     ms, _ = timed(lambda: se.set_eta_G_eta(bos, eta))
     emit({"config": "C4a", "what": "G_eta = (M^dag M)^-1 M^dag eta, 64 rhs, mixed, rtol 1e-10", "ms": ms,
           "iters": int(se.iters.max()), "relres": float(se.relres.max()), "tuned": tuned(se.solver)})
+    se16 = StochaticEstimator(L, Lt, Nrv=nrv, precision="mixed_f16", cg_rtol=1e-10, device=dev, seed=5, noise="z2")
+    ms16, _ = timed(lambda: se16.set_eta_G_eta(bos, eta))
+    emit({"config": "C4a", "what": "the same solve with p and z stored as scaled fp16 (mixed_f16)", "ms": ms16,
+          "iters": int(se16.iters.max()), "relres": float(se16.relres.max()), "tuned": tuned(se16.solver)})
+    del se16
     ms, _ = timed(lambda: se.get_bond_bond_per_b2(bos))
     emit({"config": "C4a", "what": "bond-bond correlators T1+T21+T2+T4+Tvv over the 2016 noise pairs "
                                    "(complex128, pair-field and k-space kernels around cuFFT)", "ms": ms})
@@ -936,12 +941,13 @@ def run_configs(args):
     systems = [System(L, 10 * L, 1) for L in Ls]
     phis = [ref_to_kernel(torch.tensor(pi_flux_np(rng, L, 10 * L, 1), device=dev)).reshape(-1) for L in Ls]
     rhs = [torch.randn(10 * L ** 3, dtype=torch.complex128, device=dev) / math.sqrt(2) for L in Ls]
-    s = PcgSolver(systems, mode="mixed", rtol=1e-10, max_iter=20000, device=dev, tune=True)
     args_ = (torch.cat(phis).float(), torch.cat(rhs))
-    ms, res = timed(lambda: s.solve(*args_))
-    emit({"config": "C4b", "what": "16 uneven lattices, one launch, mixed, rtol 1e-10", "ms": ms,
-          "iters_min": int(res.iters.min()), "iters_max": int(res.iters.max()),
-          "relres_max": float(res.relres.max()), "tuned": tuned(s)})
+    for mode in ("mixed", "mixed_f16"):
+        s = PcgSolver(systems, mode=mode, rtol=1e-10, max_iter=20000, device=dev, tune=True)
+        ms, res = timed(lambda: s.solve(*args_))
+        emit({"config": "C4b", "what": f"16 uneven lattices, one launch, {mode}, rtol 1e-10", "ms": ms,
+              "iters_min": int(res.iters.min()), "iters_max": int(res.iters.max()),
+              "relres_max": float(res.relres.max()), "tuned": tuned(s)})
 
     # C5: one 30-step trajectory at L=66, Ltau=660 (mixed)
     L, Lt = 66, 660
