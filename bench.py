@@ -883,7 +883,7 @@ def run_configs(args):
         ms, _ = timed(lambda: ops.apply_operator("mhm", phi_p, b_p, L, 0.1, out=out), reps=20)
         emit({"config": "C2", "what": f"M^dag M {prec}, 1 rhs (a single launch of 138,240 sites)", "ms": ms,
               "GBps": bps * N / (ms / 1e3) / 1e9})
-    for mode in ("mixed", "mixed_f16", "fp64"):
+    for mode in ("mixed", "fp64"):
         s = PcgSolver([System(L, Lt, 1)], mode=mode, rtol=1e-8, max_iter=100000, device=dev, tune=True)
         args_ = (phi.reshape(-1).to(s.angle_dtype), b.reshape(-1).to(s.vec_dtype))
         ms, res = timed(lambda: s.solve(*args_))

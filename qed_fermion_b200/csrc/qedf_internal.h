@@ -117,6 +117,7 @@ struct PcgParams {
   int max_iter, ru_interval;
   double rtol, ru_delta;
   double c1, ch, t1, th, Cb;
+  double pnorm;  // bound of the preconditioner's 2-norm: its largest absolute row sum (1 without)
   long long timeout_cycles;
   // data
   const void* phi;   // angles (float for F32/MIXED, double for F64)

@@ -142,6 +142,7 @@ struct Acc {
   double* rz;       // [2][NV]
   double* ru_rr;    // [NV]
   double* ru_rz;    // [NV]
+  double* pp;       // [2][NV] |p|^2 of the operator phase (scaled fp16 storage)
   __device__ Acc(double* a, int NV) {
     bb = a;
     pAp = a + NV;
@@ -149,9 +150,10 @@ struct Acc {
     rz = a + 5 * NV;
     ru_rr = a + 7 * NV;
     ru_rz = a + 8 * NV;
+    pp = a + 9 * NV;
   }
 };
-constexpr int ACC_PER_RHS = 9;
+constexpr int ACC_PER_RHS = 11;
 
 // unit -> system
 __device__ __forceinline__ int find_sys_A(const PcgParams& p, int u) {
@@ -537,12 +539,20 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
             X[q][c].im = fma(beta, T0[q][c].im, X[q][c].im);
             X[q][c] = round_st<SP>(X[q][c], s_pn, i_pn);
           }
+      } else if constexpr (H16) {
+        // p = z, stored at p's own scale (exact unless entries turn subnormal)
+#pragma unroll
+        for (int q = 0; q < BY; ++q)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) X[q][c] = round_st<SP>(X[q][c], s_pn, i_pn);
       }
     };
     const int tp = (a - 1 + Nt) % Nt;
     getp(X0, tp, false);
     getp(X1, a, true);
     if (E.on) E.store_st(pnew + a * sv, X1, i_pn);
+    double ppp = 0;  // |p_new|^2 over the own slices (scaled fp16 storage)
+    if constexpr (H16) ppp += sq_blk<RS, BY>(X1, E.on);
     A ang[BY][4];
     if constexpr (!PHS_S) E.load_angles(ang, phi + a * sv);
     E.phases(phi + tp * sv, t1, th);
@@ -554,6 +564,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       const int tn = (t + 1) % Nt;
       getp(X1, tn, t + 1 < bnd);
       if (E.on && t + 1 < bnd) E.store_st(pnew + tn * sv, X1, i_pn);
+      if constexpr (H16) ppp += sq_blk<RS, BY>(X1, E.on && t + 1 < bnd);
       if constexpr (!PHS_S) {
         E.phases_from(ang, t1, th);
         if (t + 1 < bnd) E.load_angles(ang, phi + (t + 1) * sv);
@@ -585,8 +596,17 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       }
       copy_blk<RS, BY>(X0, X1);
     }
-    const double sum = block_sum_d(pap, st.red);
-    if (tid == 0) atomicAdd(acc.pAp + slot * NV + v, sum);
+    if constexpr (H16) {
+      double sa = pap, sb = ppp, sc = 0;
+      block_sum3_d(sa, sb, sc, st.red);
+      if (tid == 0) {
+        atomicAdd(acc.pAp + slot * NV + v, sa);
+        atomicAdd(acc.pp + slot * NV + v, sb);
+      }
+    } else {
+      const double sum = block_sum_d(pap, st.red);
+      if (tid == 0) atomicAdd(acc.pAp + slot * NV + v, sum);
+    }
     __syncthreads();
     }
   };
@@ -669,6 +689,12 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
             X[q][c].im = fma(beta, T0[q][c].im, X[q][c].im);
             X[q][c] = round_st<SP>(X[q][c], s_pn, i_pn);
           }
+      } else if constexpr (H16) {
+        // p = z, stored at p's own scale (exact unless entries turn subnormal)
+#pragma unroll
+        for (int q = 0; q < BY; ++q)
+#pragma unroll
+          for (int c = 0; c < 2; ++c) X[q][c] = round_st<SP>(X[q][c], s_pn, i_pn);
       }
     };
     Cx<RS> X0[BY][2], X1[BY][2], Y[BY][2];
@@ -680,6 +706,8 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     wait(1);
     getp(X1, 1, true);
     if (E.on) E.store_st(pnew + a * sv, X1, i_pn);
+    double ppp = 0;  // |p_new|^2 over the own slices (scaled fp16 storage)
+    if constexpr (H16) ppp += sq_blk<RS, BY>(X1, E.on);
     A ang[BY][4];
     if constexpr (!PHS_S) E.load_angles(ang, phi + a * sv);
     E.phases(phi + tp * sv, t1, th);  // block barrier: stage 0 is read
@@ -694,6 +722,7 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       wait(i + 2);
       getp(X1, i + 2, t + 1 < bnd);
       if (E.on && t + 1 < bnd) E.store_st(pnew + tn * sv, X1, i_pn);
+      if constexpr (H16) ppp += sq_blk<RS, BY>(X1, E.on && t + 1 < bnd);
       if constexpr (!PHS_S) {
         E.phases_from(ang, t1, th);
         if (t + 1 < bnd) E.load_angles(ang, phi + (t + 1) * sv);
@@ -720,8 +749,17 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       }
       copy_blk<RS, BY>(X0, X1);
     }
-    const double sum = block_sum_d(pap, st.red);
-    if (tid == 0) atomicAdd(acc.pAp + slot * NV + v, sum);
+    if constexpr (H16) {
+      double sa = pap, sb = ppp, sc = 0;
+      block_sum3_d(sa, sb, sc, st.red);
+      if (tid == 0) {
+        atomicAdd(acc.pAp + slot * NV + v, sa);
+        atomicAdd(acc.pp + slot * NV + v, sb);
+      }
+    } else {
+      const double sum = block_sum_d(pap, st.red);
+      if (tid == 0) atomicAdd(acc.pAp + slot * NV + v, sum);
+    }
     __syncthreads();
     }
   };
@@ -1002,7 +1040,14 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
     for (int v = tid; v < NV; v += blockDim.x) {
       st.beta[v] = st.iters[v] > 0 ? st.rz[v] / st.rzold[v] : 0.0;
       if constexpr (H16)
-        if (st.active[v]) scl.p[st.iters[v] & 1][v] = scl.z[v];  // the buffer p_new goes to
+        if (st.active[v]) {
+          // the scale of the buffer p_new goes to, from a bound of its norm:
+          // |z + beta p_old| <= |P| |r| + beta |p_old| (|p_old| measured in the
+          // last operator phase); p grows far above r in ill-conditioned solves
+          double est = p.pnorm * sqrt(st.rr[v]);
+          if (st.iters[v] > 0) est += fabs(st.beta[v]) * sqrt(acc.pp[((it & 1) ^ 1) * NV + v]);
+          scl.p[st.iters[v] & 1][v] = st_scale(est * est);
+        }
     }
     __syncthreads();
     // (the guess pass uses the pAp slot of odd iterations, so that its BC
@@ -1040,8 +1085,11 @@ __global__ void __launch_bounds__(MaxT<BY, ECS>::value, MaxT<BY, ECS>::min_block
       unitE(u, s, v, c0, c1);
       if (st.active[v]) elementwise(1, u, slot ^ 1);
     }
-    if (blockIdx.x == 0)  // pAp slot of the next iteration
-      for (int v = tid; v < NV; v += blockDim.x) acc.pAp[(aslot ^ 1) * NV + v] = 0;
+    if (blockIdx.x == 0)  // pAp (and |p|^2) slot of the next iteration
+      for (int v = tid; v < NV; v += blockDim.x) {
+        acc.pAp[(aslot ^ 1) * NV + v] = 0;
+        if constexpr (H16) acc.pp[(aslot ^ 1) * NV + v] = 0;
+      }
     pc.lap(3);
     if (!(ok = grid_barrier(p.bar, nblk, budget, bar_target))) break;
     pc.lap(4);
@@ -1210,6 +1258,17 @@ int pcg_plan(PcgParams& p, const qedf_system* sys, int nsys, const qedf_pcg_opts
   p.t1 = f.t1;
   p.th = f.th;
   p.Cb = f.Cb;
+  // largest absolute row sum of the systems' preconditioners (a bound of its
+  // 2-norm, P being symmetric); 1 for the identity
+  p.pnorm = 1.0;
+  for (int s = 0; s < nsys; ++s) {
+    if (!p.sys[s].precon) continue;
+    for (int t = 0; t < p.sys[s].Nt; ++t) {
+      double row = 0;
+      pre_row(h_pre, p.sys[s].Nt, t, [&](int, float val) { row += std::fabs((double)val); });
+      p.pnorm = std::max(p.pnorm, row);
+    }
+  }
   return QEDF_OK;
 }
 

@@ -471,6 +471,17 @@ __device__ __forceinline__ void axpy_blk(Cx<R> (&y)[BY][2], const Cx<R> (&a)[BY]
     }
 }
 
+// sum of |a|^2 over a block, in double (0 when !on)
+template <typename R, int BY>
+__device__ __forceinline__ double sq_blk(const Cx<R> (&a)[BY][2], bool on) {
+  R s = 0;
+#pragma unroll
+  for (int r = 0; r < BY; ++r)
+#pragma unroll
+    for (int c = 0; c < 2; ++c) s = fma(a[r][c].re, a[r][c].re, fma(a[r][c].im, a[r][c].im, s));
+  return on ? (double)s : 0.0;
+}
+
 template <typename R, int BY>
 __device__ __forceinline__ void copy_blk(Cx<R> (&y)[BY][2], const Cx<R> (&a)[BY][2]) {
 #pragma unroll
