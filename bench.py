@@ -454,9 +454,10 @@ def run_native(args):
         result["pcg_share_of_step"] = pcg_time / elapsed
         result["cg_iters_per_solve"] = statistics.mean(iters_all) if iters_all else None
 
-    # --- end to end through the public API with host buffers
+    # --- end to end through the public API with host buffers (every rank, the
+    # whole job's trajectories over the slowest rank's time)
     e2e = None
-    if rank == 0 and not args.quick:
+    if not args.quick:
         hb = torch.empty((bs, 2, L, L, Lt), dtype=torch.float32, pin_memory=True)
         hb.copy_(hmc.boson.cpu())
         hout = torch.empty_like(hb).pin_memory()
@@ -476,7 +477,10 @@ def run_native(args):
         e1.record(stream)
         torch.cuda.synchronize()
         t_e2e = e0.elapsed_time(e1) / 1e3
-        e2e = {"value": 3600.0 * k_e2e * bs / t_e2e, "unit": UNIT, "h2d_bytes_per_step": hb.numel() * 4,
+        if world > 1:
+            dist.barrier()
+        t_e2e, v_e2e = aggregate_over_ranks(t_e2e, k_e2e * bs, world, dist, dev)
+        e2e = {"value": v_e2e, "unit": UNIT, "h2d_bytes_per_step": hb.numel() * 4,
                "d2h_bytes_per_step": hout.numel() * 4 + hH.numel() * 8, "steps": k_e2e}
 
     def time_trajectories(h, n):
@@ -498,7 +502,7 @@ def run_native(args):
 
     # --- plain FP64 path, same workload
     fp64 = None
-    if rank == 0 and args.fp64_steps > 0 and not args.quick:
+    if rank == 0 and world == 1 and args.fp64_steps > 0 and not args.quick:
         h64 = make("fp64")
         h64.boson = hmc.boson.to(torch.float64)
         fp64 = time_trajectories(h64, args.fp64_steps)
@@ -517,7 +521,7 @@ def run_native(args):
     # --- the same trajectories replayed from a CUDA graph (one graph launch per
     # trajectory; the first proposal, in the warm-up, captures it)
     graph = None
-    if rank == 0 and args.graph_steps > 0 and not args.quick:
+    if rank == 0 and world == 1 and args.graph_steps > 0 and not args.quick:
         hg = make("mixed", graph=True)
         hg.boson = hmc.boson.clone()
         graph = time_trajectories(hg, args.graph_steps)
@@ -527,7 +531,7 @@ def run_native(args):
     # --- the leapfrog's solves started from the linear extrapolation of the
     # previous two solutions instead of zero
     chrono = None
-    if rank == 0 and args.chrono_steps > 0 and not args.quick:
+    if rank == 0 and world == 1 and args.chrono_steps > 0 and not args.quick:
         hc = make("mixed", chrono_guess="linear")
         hc.boson = hmc.boson.clone()
         chrono = time_trajectories(hc, args.chrono_steps)
@@ -537,7 +541,7 @@ def run_native(args):
 
     # --- bf16 vector storage, same workload
     bf16 = None
-    if rank == 0 and args.bf16_steps > 0 and not args.quick:
+    if rank == 0 and world == 1 and args.bf16_steps > 0 and not args.quick:
         hb16 = make("mixed_bf16")
         hb16.boson = hmc.boson.clone()
         bf16 = time_trajectories(hb16, args.bf16_steps)
@@ -548,7 +552,7 @@ def run_native(args):
 
     # --- scaled fp16 vector storage, same workload
     f16 = None
-    if rank == 0 and args.f16_steps > 0 and not args.quick:
+    if rank == 0 and world == 1 and args.f16_steps > 0 and not args.quick:
         hf16 = make("mixed_f16")
         hf16.boson = hmc.boson.clone()
         f16 = time_trajectories(hf16, args.f16_steps)
@@ -559,7 +563,7 @@ def run_native(args):
 
     # --- Delta H of one shared trajectory: mixed and bf16 storage against FP64
     dH = None
-    if rank == 0 and not args.quick:
+    if rank == 0 and world == 1 and not args.quick:
         gen = torch.Generator(device=dev)
         gen.manual_seed(seed + 7)
         x0 = hmc.boson.to(torch.float64)
@@ -582,7 +586,7 @@ def run_native(args):
     # --- acceptance, mixed against FP64, at a step where proposals are accepted:
     # both chains take the same momenta, pseudofermions and uniforms each step
     acc = None
-    if rank == 0 and args.accept_steps > 0 and not args.quick:
+    if rank == 0 and world == 1 and args.accept_steps > 0 and not args.quick:
         from qed_fermion_b200.hmc import metropolis_accept
         gen = torch.Generator(device=dev)
         gen.manual_seed(seed + 11)
@@ -619,7 +623,7 @@ def run_native(args):
 
     # --- M^dag M matvec bandwidth (several right-hand sides, working set > L2)
     mhm = None
-    if rank == 0 and args.mhm_rhs > 0 and not args.quick:
+    if rank == 0 and world == 1 and args.mhm_rhs > 0 and not args.quick:
         nr = args.mhm_rhs
         mhm = {}
         for prec, cdt, rdt, bps in (("c64", torch.complex64, torch.float32, 24), ("c128", torch.complex128,
