@@ -583,43 +583,46 @@ def run_native(args):
                         "rel_err_vs_H0": ((dHm - dHd).abs() / H0d.abs().cpu()).tolist(),
                         "rel_err_vs_dH": ((dHm - dHd).abs() / dHd.abs()).tolist()}
 
-    # --- acceptance, mixed against FP64, at a step where proposals are accepted:
-    # both chains take the same momenta, pseudofermions and uniforms each step
+    # --- acceptance, mixed (float and scaled fp16 storage) against FP64, at a
+    # step where proposals are accepted: all chains take the same momenta,
+    # pseudofermions and uniforms each step
     acc = None
     if rank == 0 and world == 1 and args.accept_steps > 0 and not args.quick:
         from qed_fermion_b200.hmc import metropolis_accept
         gen = torch.Generator(device=dev)
         gen.manual_seed(seed + 11)
-        hm = make("mixed")
-        hd = make("fp64")
-        hm.delta_t_tensor.fill_(args.accept_delta_t)
-        hd.delta_t_tensor.fill_(args.accept_delta_t)
-        xm = hmc.boson.to(torch.float32).clone()
-        xd = xm.to(torch.float64)
-        rec = {"mixed": [], "fp64": []}
-        nmis, dd = 0, []
+        chains = {"fp64": make("fp64"), "mixed": make("mixed"), "mixed_f16": make("mixed_f16")}
+        xs = {}
+        for k, h in chains.items():
+            h.delta_t_tensor.fill_(args.accept_delta_t)
+            xs[k] = hmc.boson.to(torch.float32).clone().to(h.dtype)
+        rec = {k: [] for k in chains}
+        nmis = {k: 0 for k in chains if k != "fp64"}
+        dd = {k: [] for k in nmis}
         for _ in range(args.accept_steps):
-            p0 = torch.randn(xd.shape, device=dev, dtype=torch.float64, generator=gen).to(torch.float32)
+            p0 = torch.randn(xs["fp64"].shape, device=dev, dtype=torch.float64, generator=gen).to(torch.float32)
             R = torch.randn((bs, N), device=dev, dtype=torch.complex128, generator=gen) / math.sqrt(2)
             u = torch.rand(bs, device=dev, dtype=torch.float64, generator=gen)
-            nm, H0m, H1m, _, _ = hm.leapfrog_proposer5(xm, p0=p0, R=R)
-            nd, H0d, H1d, _, _ = hd.leapfrog_proposer5(xd, p0=p0.to(torch.float64), R=R)
-            am, _ = metropolis_accept(H0m, H1m, u)
-            ad, _ = metropolis_accept(H0d, H1d, u)
-            xm = torch.where(am.view(-1, 1, 1, 1, 1), nm.to(torch.float32), xm)
-            xd = torch.where(ad.view(-1, 1, 1, 1, 1), nd.to(torch.float64), xd)
-            rec["mixed"].append(((H1m - H0m).cpu(), am.cpu()))
-            rec["fp64"].append(((H1d - H0d).cpu(), ad.cpu()))
-            nmis += int((am != ad).sum())
-            dd.append(((H1m - H0m) - (H1d - H0d)).abs().cpu())
+            step = {}
+            for k, h in chains.items():
+                nx, H0, H1, _, _ = h.leapfrog_proposer5(xs[k], p0=p0.to(h.dtype), R=R)
+                a, _ = metropolis_accept(H0, H1, u)
+                xs[k] = torch.where(a.view(-1, 1, 1, 1, 1), nx.to(h.dtype), xs[k])
+                step[k] = (H1 - H0, a)
+                rec[k].append(((H1 - H0).cpu(), a.cpu()))
+            for k in nmis:
+                nmis[k] += int((step[k][1] != step["fp64"][1]).sum())
+                dd[k].append((step[k][0] - step["fp64"][0]).abs().cpu())
         acc = {"delta_t": args.accept_delta_t, "n_leapfrog": args.n_leapfrog, "steps": args.accept_steps,
-               "chains": bs, "decisions_differing": nmis,
-               "max_abs_dH_difference": float(torch.stack(dd).max())}
+               "chains": bs, "decisions_differing": nmis["mixed"],
+               "max_abs_dH_difference": float(torch.stack(dd["mixed"]).max()),
+               "mixed_f16_vs_fp64": {"decisions_differing": nmis["mixed_f16"],
+                                     "max_abs_dH_difference": float(torch.stack(dd["mixed_f16"]).max())}}
         for k, v in rec.items():
             d = torch.stack([a for a, _ in v]).double()
             acc[k] = {"acceptance": float(torch.stack([b for _, b in v]).double().mean()),
                       "mean_exp_minus_dH": float(torch.exp(-d).mean()), "mean_dH": float(d.mean())}
-        del hm, hd
+        del chains
 
     # --- M^dag M matvec bandwidth (several right-hand sides, working set > L2)
     mhm = None
