@@ -826,20 +826,26 @@ def run_kernels(args):
         S_b = torch.zeros(L * L, dtype=torch.complex128, device=dev)
         ms = timed(lambda: ops.bb_kspace_acc(fa_b, fb_b, S_b))
         emit(f"k_bb_kspace_acc ({prec})", f"{len(prs)} pairs x {Lt} slices", ms, len(prs) * N * 2 * sv)
-        del eta_b, g_b, fa_b, fb_b
+        v_b = torch.empty_like(eta_b)
+        tv_b = torch.zeros(L * L, dtype=torch.complex128, device=dev)
+        ms = timed(lambda: ops.bb_vfield(eta_b, g_b, ep_b, L, v_b, tv_b))
+        emit(f"k_bb_vfield ({prec})", f"{nrv} vectors", ms, (3 * nrv + 1) * N * sv)
+        ms = timed(lambda: ops.bb_diag(eta_b, g_b, ep_b, L))
+        emit(f"k_bb_diag ({prec})", f"{nrv} vectors", ms, (2 * nrv + 1) * N * sv)
+        del eta_b, g_b, fa_b, fb_b, v_b
         pm = torch.zeros_like(ang)
         fm = torch.ones_like(ang)
         dt = torch.full((bs,), 0.01, dtype=torch.float64, device=dev)
         ms = timed(lambda: ops.kick_drift(pm, fm, ang, dt, None, 0.5, 1.0, L))
         emit(f"k_kick_drift ({prec})", f"{bs} fields, kick and drift", ms, bs * N * 2 * sp * 5)
     nb = 2
-    for mode in ("mixed", "fp64"):
+    for mode in ("mixed", "mixed_f16", "fp64"):
         s = PcgSolver([System(L, Lt, nb)], mode=mode, rtol=0.0, max_iter=100, device=dev)
         a_ = ref_to_kernel(boson[:nb]).reshape(-1).to(s.angle_dtype)
         b_ = torch.randn(nb * N, dtype=torch.complex128, device=dev).to(s.vec_dtype)
         ms = timed(lambda: s.solve(a_, b_), reps=2, graph=False)
-        sv = 8 if mode == "mixed" else 16
-        emit(f"k_pcg ({mode})", f"100 iterations, {nb} rhs", ms, 100 * nb * N * (7 * sv + 2 * (sv // 2)))
+        bps = {"mixed": 64, "mixed_f16": 48, "fp64": 128}[mode]  # the algorithmic model per site-iteration
+        emit(f"k_pcg ({mode})", f"100 iterations, {nb} rhs", ms, 100 * nb * N * bps)
     return 0
 
 

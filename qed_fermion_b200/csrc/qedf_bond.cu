@@ -161,21 +161,23 @@ __global__ void __launch_bounds__(256) k_bb_kspace_acc(const R* A, const R* B, i
 // Tvv's current field of each noise vector s (stochastic_estimator.py:1612-1652),
 //   v_s(r) = g_s(r+x) conj(eta_s(r)) e^{i phi_x(r)} + g_s(r) conj(eta_s(r+x)) e^{-i phi_x(r)},
 // written for every slice, and its sum over vectors and slices per site,
-// added to Tv[Vs] (complex, double).  Grid (site blocks, vectors); a thread
-// walks its site through all slices, so the sum needs one atomic per site
-// and vector.
+// added to Tv[Vs] (complex, double).  Grid (site blocks, vectors, slice
+// ranges): a thread walks its site through one range of slices, so the sum
+// needs one atomic per site, vector and range; the ranges give the grid
+// enough blocks to fill the SMs when Vs x Nrv alone does not.
 template <typename R>
-__global__ void __launch_bounds__(256) k_bb_vfield(const R* eta, const R* g, const R* ep, int L, int Nt, R* v,
-                                                   double* Tv) {
+__global__ void __launch_bounds__(256) k_bb_vfield(const R* eta, const R* g, const R* ep, int L, int Nt, int tlen,
+                                                   R* v, double* Tv) {
   const int Vs = L * L;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   const int s = blockIdx.y;
+  const int t0 = blockIdx.z * tlen, t1 = min(t0 + tlen, Nt);
   if (r >= Vs) return;
   const int x = r % L, y = r / L;
   const int r1 = y * L + (x + 1 == L ? 0 : x + 1);
   const int64_t base = (int64_t)s * Nt * Vs;
   double sr = 0, si = 0;
-  for (int t = 0; t < Nt; ++t) {
+  for (int t = t0; t < t1; ++t) {
     const int64_t o = base + (int64_t)t * Vs;
     const Cx<R> e = ldcx(ep, (int64_t)t * Vs + r);
     const Cx<R> val = cmul(cmul(ldcx(g, o + r1), conjc(ldcx(eta, o + r))), e) +
@@ -184,8 +186,10 @@ __global__ void __launch_bounds__(256) k_bb_vfield(const R* eta, const R* g, con
     sr += (double)val.re;
     si += (double)val.im;
   }
-  atomicAdd(Tv + 2 * r, sr);
-  atomicAdd(Tv + 2 * r + 1, si);
+  if (t1 > t0) {
+    atomicAdd(Tv + 2 * r, sr);
+    atomicAdd(Tv + 2 * r + 1, si);
+  }
 }
 
 // The short-distance terms the correlators add to their pair sums, summed
@@ -193,31 +197,34 @@ __global__ void __launch_bounds__(256) k_bb_vfield(const R* eta, const R* g, con
 //   D[0] = sum g_s(r+x) conj(eta_s(r-x)) e^{i phi_x(r)} e^{i phi_x(r-x)}     (T1, at d = -x)
 //   D[1] = sum g_s(r) conj(eta_s(r))                                         (T21 and T2, at d = 0)
 //   D[2] = sum g_s(r) conj(eta_s(r+2x)) e^{-i phi_x(r)} e^{-i phi_x(r+x)}   (T4, at d = +x)
+// Blocks take (vector, slice) rows in turn (grid y) and the sites of a row
+// (grid x), so no thread divides a 64-bit index.
 template <typename R>
 __global__ void __launch_bounds__(256) k_bb_diag(const R* eta, const R* g, const R* ep, int Nrv, int L, int Nt,
                                                  double* D) {
   __shared__ double red[6][8];
   const int Vs = L * L;
-  const int64_t n = (int64_t)Nrv * Nt * Vs;
+  const int rows = Nrv * Nt;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int r = (int)(i % Vs);
-    const int64_t st = i - r;  // (vector, slice) offset
-    const int tslice = (int)((i / Vs) % Nt);
-    const int x = r % L, y = r / L;
-    const int xm = x == 0 ? L - 1 : x - 1, xp = x + 1 == L ? 0 : x + 1, xpp = xp + 1 == L ? 0 : xp + 1;
+  for (int q = blockIdx.y; q < rows; q += gridDim.y) {
+    const int tslice = q % Nt;
+    const int64_t st = (int64_t)q * Vs;             // (vector, slice) offset
     const int64_t et = (int64_t)tslice * Vs;
-    const Cx<R> e = ldcx(ep, et + r), em1 = ldcx(ep, et + y * L + xm), ep1 = ldcx(ep, et + y * L + xp);
-    const Cx<R> gr = ldcx(g, i);
-    const Cx<R> d0 = cmul(cmul(ldcx(g, st + y * L + xp), conjc(ldcx(eta, st + y * L + xm))), cmul(e, em1));
-    const Cx<R> d1 = cmul(gr, conjc(ldcx(eta, i)));
-    const Cx<R> d2 = cmul(cmul(gr, conjc(ldcx(eta, st + y * L + xpp))), conjc(cmul(e, ep1)));
-    acc[0] += d0.re;
-    acc[1] += d0.im;
-    acc[2] += d1.re;
-    acc[3] += d1.im;
-    acc[4] += d2.re;
-    acc[5] += d2.im;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < Vs; r += gridDim.x * blockDim.x) {
+      const int x = r % L, y = r / L;
+      const int xm = x == 0 ? L - 1 : x - 1, xp = x + 1 == L ? 0 : x + 1, xpp = xp + 1 == L ? 0 : xp + 1;
+      const Cx<R> e = ldcx(ep, et + r), em1 = ldcx(ep, et + y * L + xm), ep1 = ldcx(ep, et + y * L + xp);
+      const Cx<R> gr = ldcx(g, st + r);
+      const Cx<R> d0 = cmul(cmul(ldcx(g, st + y * L + xp), conjc(ldcx(eta, st + y * L + xm))), cmul(e, em1));
+      const Cx<R> d1 = cmul(gr, conjc(ldcx(eta, st + r)));
+      const Cx<R> d2 = cmul(cmul(gr, conjc(ldcx(eta, st + y * L + xpp))), conjc(cmul(e, ep1)));
+      acc[0] += d0.re;
+      acc[1] += d0.im;
+      acc[2] += d1.re;
+      acc[3] += d1.im;
+      acc[4] += d2.re;
+      acc[5] += d2.im;
+    }
   }
   const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
 #pragma unroll
@@ -239,16 +246,26 @@ int vfield_entry(const R* eta, const R* g, const R* ep, int Nrv, int Lx, int Lta
                  cudaStream_t st) {
   if (!eta || !g || !ep || !v || !Tv || Nrv < 1 || Nrv > 65535 || Lx < 2 || Ltau < 1) return QEDF_ERR_ARG;
   const int Vs = Lx * Lx;
-  k_bb_vfield<R><<<dim3((Vs + 255) / 256, Nrv), 256, 0, st>>>(eta, g, ep, Lx, Ltau, v, Tv);
+  // split the slices so that the grid holds about four blocks per SM
+  const int64_t base_blocks = (int64_t)((Vs + 255) / 256) * Nrv;
+  const int64_t want = (int64_t)num_sms() * 4;
+  const int64_t split = std::max<int64_t>(1, (want + base_blocks - 1) / base_blocks);
+  const int nsplit = (int)std::min<int64_t>(std::min<int64_t>(Ltau, 65535), split);
+  const int tlen = (Ltau + nsplit - 1) / nsplit;
+  const int nz = (Ltau + tlen - 1) / tlen;
+  k_bb_vfield<R><<<dim3((Vs + 255) / 256, Nrv, nz), 256, 0, st>>>(eta, g, ep, Lx, Ltau, tlen, v, Tv);
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
 
 template <typename R>
 int diag_entry(const R* eta, const R* g, const R* ep, int Nrv, int Lx, int Ltau, double* D, cudaStream_t st) {
   if (!eta || !g || !ep || !D || Nrv < 1 || Lx < 3 || Ltau < 1) return QEDF_ERR_ARG;
-  const int64_t n = (int64_t)Nrv * Ltau * Lx * Lx;
-  const int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)num_sms() * 4);
-  k_bb_diag<R><<<(unsigned)blocks, 256, 0, st>>>(eta, g, ep, Nrv, Lx, Ltau, D);
+  const int Vs = Lx * Lx;
+  const int gx = std::min((Vs + 255) / 256, 65535);  // one pass over a row's sites
+  const int64_t rows = (int64_t)Nrv * Ltau;
+  if (rows > INT32_MAX) return QEDF_ERR_SIZE;
+  const int gy = (int)std::min<int64_t>(rows, std::max(1, num_sms() * 4 / gx));
+  k_bb_diag<R><<<dim3(gx, std::min(gy, 65535)), 256, 0, st>>>(eta, g, ep, Nrv, Lx, Ltau, D);
   return cudaGetLastError() == cudaSuccess ? QEDF_OK : QEDF_ERR_CUDA;
 }
 
