@@ -197,8 +197,8 @@ __global__ void __launch_bounds__(256) k_bb_vfield(const R* eta, const R* g, con
 //   D[0] = sum g_s(r+x) conj(eta_s(r-x)) e^{i phi_x(r)} e^{i phi_x(r-x)}     (T1, at d = -x)
 //   D[1] = sum g_s(r) conj(eta_s(r))                                         (T21 and T2, at d = 0)
 //   D[2] = sum g_s(r) conj(eta_s(r+2x)) e^{-i phi_x(r)} e^{-i phi_x(r+x)}   (T4, at d = +x)
-// Blocks take (vector, slice) rows in turn (grid y) and the sites of a row
-// (grid x), so no thread divides a 64-bit index.
+// Blocks take (vector, slice) rows in turn (grid y), one thread per site of a
+// row (grid x), so no thread divides a 64-bit index.
 template <typename R>
 __global__ void __launch_bounds__(256) k_bb_diag(const R* eta, const R* g, const R* ep, int Nrv, int L, int Nt,
                                                  double* D) {
@@ -206,18 +206,22 @@ __global__ void __launch_bounds__(256) k_bb_diag(const R* eta, const R* g, const
   const int Vs = L * L;
   const int rows = Nrv * Nt;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  for (int q = blockIdx.y; q < rows; q += gridDim.y) {
-    const int tslice = q % Nt;
-    const int64_t st = (int64_t)q * Vs;             // (vector, slice) offset
-    const int64_t et = (int64_t)tslice * Vs;
-    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < Vs; r += gridDim.x * blockDim.x) {
-      const int x = r % L, y = r / L;
-      const int xm = x == 0 ? L - 1 : x - 1, xp = x + 1 == L ? 0 : x + 1, xpp = xp + 1 == L ? 0 : xp + 1;
-      const Cx<R> e = ldcx(ep, et + r), em1 = ldcx(ep, et + y * L + xm), ep1 = ldcx(ep, et + y * L + xp);
+  // one site per thread (the grid's x extent covers a row); rows in turn,
+  // four in flight
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < Vs) {
+    const int x = r % L, y = r / L;
+    const int xm = x == 0 ? L - 1 : x - 1, xp = x + 1 == L ? 0 : x + 1, xpp = xp + 1 == L ? 0 : xp + 1;
+    const int rm = y * L + xm, rp = y * L + xp, rpp = y * L + xpp;
+#pragma unroll 4
+    for (int q = blockIdx.y; q < rows; q += gridDim.y) {
+      const int64_t st = (int64_t)q * Vs;               // (vector, slice) offset
+      const int64_t et = (int64_t)(q % Nt) * Vs;
+      const Cx<R> e = ldcx(ep, et + r), em1 = ldcx(ep, et + rm), ep1 = ldcx(ep, et + rp);
       const Cx<R> gr = ldcx(g, st + r);
-      const Cx<R> d0 = cmul(cmul(ldcx(g, st + y * L + xp), conjc(ldcx(eta, st + y * L + xm))), cmul(e, em1));
+      const Cx<R> d0 = cmul(cmul(ldcx(g, st + rp), conjc(ldcx(eta, st + rm))), cmul(e, em1));
       const Cx<R> d1 = cmul(gr, conjc(ldcx(eta, st + r)));
-      const Cx<R> d2 = cmul(cmul(gr, conjc(ldcx(eta, st + y * L + xpp))), conjc(cmul(e, ep1)));
+      const Cx<R> d2 = cmul(cmul(gr, conjc(ldcx(eta, st + rpp))), conjc(cmul(e, ep1)));
       acc[0] += d0.re;
       acc[1] += d0.im;
       acc[2] += d1.re;
@@ -261,7 +265,8 @@ template <typename R>
 int diag_entry(const R* eta, const R* g, const R* ep, int Nrv, int Lx, int Ltau, double* D, cudaStream_t st) {
   if (!eta || !g || !ep || !D || Nrv < 1 || Lx < 3 || Ltau < 1) return QEDF_ERR_ARG;
   const int Vs = Lx * Lx;
-  const int gx = std::min((Vs + 255) / 256, 65535);  // one pass over a row's sites
+  if ((Vs + 255) / 256 > 65535) return QEDF_ERR_SIZE;
+  const int gx = (Vs + 255) / 256;  // one thread per site of a row
   const int64_t rows = (int64_t)Nrv * Ltau;
   if (rows > INT32_MAX) return QEDF_ERR_SIZE;
   const int gy = (int)std::min<int64_t>(rows, std::max(1, num_sms() * 4 / gx));
