@@ -43,3 +43,36 @@ def test_tau_block_update_moves_only_its_block():
     h.metropolis_update()
     assert [len(q) for q in h.threshold_queue] == [2, 2] and h.tau_block_idx == 0
     assert all(0.0 <= v <= 1.0 for q in h.threshold_queue for v in q)
+
+
+def test_threshold_queue_reads_pending_entries_in_order():
+    """Proposals leave their clipped acceptance probabilities on the device;
+    reading the queue appends them in order, and entries older than the
+    queue's length (which the deque would drop anyway) are not kept pending."""
+    h = HmcSampler(Lx=4, Ltau=40, bs=2, device="cpu", max_tau_block_idx=1)
+    maxlen = h.threshold_queue[0].maxlen
+    for k in range(maxlen + 3):
+        h._thr_pending.append(torch.tensor([k / 100, 1 - k / 100], dtype=torch.float64))
+        del h._thr_pending[:-maxlen]
+    assert len(h._thr_pending) == maxlen
+    q = h.threshold_queue
+    assert list(q[0]) == pytest.approx([k / 100 for k in range(3, maxlen + 3)])
+    assert list(q[1]) == pytest.approx([1 - k / 100 for k in range(3, maxlen + 3)])
+    assert h._thr_pending == []
+
+
+def test_sampler_option_validation():
+    with pytest.raises(ValueError):
+        HmcSampler(Lx=4, Ltau=40, bs=1, device="cpu", chrono_guess="quadratic")
+    with pytest.raises(ValueError):
+        HmcSampler(Lx=4, Ltau=40, bs=1, device="cpu", precision="bf16")
+    h = HmcSampler(Lx=4, Ltau=40, bs=1, device="cpu", chrono_guess="linear", graph=True, precision="mixed_f16")
+    assert h.chrono_guess == "linear" and h.use_graph and h.solver.mode == "mixed_f16"
+    # the guesses along a trajectory: none for the first solve, then the last
+    # solution or the linear extrapolation of the last two
+    a, b = torch.tensor([1.0, 2.0]), torch.tensor([3.0, 5.0])
+    assert h._chrono_guess([]) is None
+    assert torch.equal(h._chrono_guess([a]), a)
+    assert torch.equal(h._chrono_guess([a, b]), 2 * b - a)
+    h.chrono_guess = "last"
+    assert torch.equal(h._chrono_guess([a, b]), b)
