@@ -91,8 +91,8 @@ def test_operator_replays_in_cuda_graph():
     assert torch.equal(out, want)
 
 
-@pytest.mark.parametrize("precision", ["mixed", "fp64"])
-def test_trajectory_graph_matches_eager(precision):
+@pytest.mark.parametrize("precision,chrono", [("mixed", None), ("fp64", None), ("mixed_f16", "linear")])
+def test_trajectory_graph_matches_eager(precision, chrono):
     """Metropolis updates with the trajectory replayed from a CUDA graph give
     the eager sampler's fields, Hamiltonians and decisions: same seed, so the
     same draws; the first proposal runs eagerly and captures, the later ones
@@ -101,7 +101,7 @@ def test_trajectory_graph_matches_eager(precision):
     from qed_fermion_b200.hmc import HmcSampler
     dev = torch.device("cuda:0")
     kw = dict(Lx=6, Ltau=60, bs=2, delta_t=0.02, N_leapfrog=3, precision=precision, cg_rtol=1e-10,
-              device=dev, seed=7, max_tau_block_idx=1, autotune=False)
+              device=dev, seed=7, max_tau_block_idx=1, autotune=False, chrono_guess=chrono)
     runs = {}
     for graph in (False, True):
         h = HmcSampler(graph=graph, **kw)
