@@ -64,6 +64,8 @@ def parse_args(argv=None):
                     help="trajectories timed with the PCG's vectors stored as bf16 (mixed arithmetic)")
     ap.add_argument("--f16-steps", type=int, default=5,
                     help="trajectories timed with the PCG's vectors stored as scaled fp16 (mixed arithmetic)")
+    ap.add_argument("--options-steps", type=int, default=5,
+                    help="trajectories timed with fp16 storage, chronological guesses and graph replay together")
     ap.add_argument("--graph-steps", type=int, default=10,
                     help="trajectories timed with each trajectory replayed from a CUDA graph (mixed)")
     ap.add_argument("--chrono-steps", type=int, default=10,
@@ -518,6 +520,17 @@ def run_native(args):
                                       "complex128")
             del hd
 
+    # --- every option at once: fp16 storage, linear chronological guesses and
+    # trajectories replayed from a CUDA graph
+    fastest = None
+    if rank == 0 and world == 1 and args.options_steps > 0 and not args.quick:
+        ho = make("mixed_f16", graph=True, chrono_guess="linear")
+        ho.boson = hmc.boson.clone()
+        fastest = time_trajectories(ho, args.options_steps)
+        fastest["path"] = ("mixed precision with p and z stored as scaled fp16, linear chronological initial "
+                           "guesses and trajectories replayed from a CUDA graph")
+        del ho
+
     # --- the same trajectories replayed from a CUDA graph (one graph launch per
     # trajectory; the first proposal, in the warm-up, captures it)
     graph = None
@@ -663,7 +676,7 @@ def run_native(args):
                "s_per_unit": u}
 
     if rank == 0:
-        for leg in (f16, bf16, graph, chrono):
+        for leg in (f16, bf16, graph, chrono, fastest):
             if leg and fp64:
                 leg["speedup_vs_fp64"] = leg["value"] / fp64["value"]
         line = {
@@ -686,7 +699,7 @@ def run_native(args):
                                        if fp64 and "dropin" in fp64 else None),
             "pcg_launch_shape": ({k: hmc.solver.tuned[k] for k in ("by", "slab", "stage", "chunk")}
                                  if hmc.solver.tuned else None),
-            "bf16": bf16, "f16": f16, "graph": graph, "chrono": chrono, "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate,
+            "bf16": bf16, "f16": f16, "all_options": fastest, "graph": graph, "chrono": chrono, "delta_H": dH, "mhm_matvec": mhm, "acceptance": acc_rate,
             "acceptance_vs_fp64": acc, **result,
         }
         print(json.dumps(line), flush=True)
